@@ -1,0 +1,344 @@
+"""Benchmark: STEM probe*slices/s of the fused multislice engine on one or more B200s.
+
+Workload (``--workload stem-adf``, the default): SrTiO3 [001], 8x8x50 unit cells, 2 slices per
+cell (100 slices), Peng parameters, 300 kV, 25 mrad probe with C3 = -5 um, 64x64 raster at
+0.5 Angstrom (8 px at 0.0625 Angstrom/px), 512^2 window, 1024^2 potential grid, ADF 60-200 mrad and
+BF 0-10 mrad detectors.  Synthetic (seeded) structure; no dataset.
+
+One "step" is one complete STEM request on the device: transmission build (potential, FFT,
+exp) + slice loop for all 4096 probes + detector reduction, inputs already resident in HBM.
+``value`` = probe*slices per second over all ranks (weak scaling: every rank runs its own
+request).  ``e2e`` = the same metric through ``totem_stem_run`` with host buffers (upload,
+run, download every step).
+
+``--impl reference`` times the FP64 CPU oracle (the NumPy restatement of the reference's CPU
+path; MATLAB is not available) on a bounded sample of the same workload with all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_ELEM = 8  # complex64
+
+
+def build_workload(name: str, seed: int | None = None):
+    from totem_b200 import request
+    if name == "stem-adf":
+        return request.build_srtio3_stem(phonon_seed=seed)
+    if name == "stem-adf-small":
+        return request.build_srtio3_stem(cells=(4, 4, 10), n=256, raster=(32, 32), sampling=0.0625, step=8)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [ln.strip().split(", ") for ln in self.f.read().splitlines() if ln.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU sample (oracle) -- used for cpu_baseline and for --impl reference
+# ----------------------------------------------------------------------------------------------
+
+def _potential_chunk(args):
+    req, lo, hi = args
+    from oracle import stem_oracle as so
+    import copy
+    r = copy.copy(req)
+    r.ele_n = req.ele_n[lo:hi]
+    r.series_n = np.array([hi - lo], dtype=float)
+    r.ele_n_i = req.ele_n_i[:0]
+    r.series_n_i = np.array([0.0])
+    return so.potential_fourier(r)[0]
+
+
+def _loop_sample(args):
+    psi, T, r0, c0, prop = args
+    import scipy.fft as sfft
+    for k in range(T.shape[0]):
+        psi = psi * T[k, r0:r0 + psi.shape[0], c0:c0 + psi.shape[1]]
+        psi = sfft.ifft2(sfft.fft2(psi) * prop)
+    return float(np.abs(psi).sum())
+
+
+def cpu_sample(req, workers: int, sample_slices: int = 2):
+    """Time the oracle on a bounded sample and extrapolate to the full request.
+
+    (a) the potential + transmission of one slice (its atoms split over ``workers`` processes);
+    (b) ``workers`` probes through ``sample_slices`` slices each, in parallel.
+    Full-request CPU time = slices * t(a) + probe_slices / rate(b).
+    """
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from oracle import stem_oracle as so
+    import copy
+    ctx = mp.get_context("spawn")
+    n0 = int(req.padded_series()[0][0])
+    bounds = np.linspace(0, n0, workers + 1).astype(int)
+    one = copy.copy(req)
+    one.ele_n = req.ele_n[:n0]
+    with ProcessPoolExecutor(workers, mp_context=ctx) as ex:
+        list(ex.map(_potential_chunk, [(one, 0, 1)] * workers))  # warm the workers up
+        t0 = time.perf_counter()
+        parts = list(ex.map(_potential_chunk, [(one, int(bounds[i]), int(bounds[i + 1])) for i in range(workers)]))
+        vg = np.sum(parts, axis=0)[None]
+        one.series_n = np.array([n0], dtype=float)
+        one.series_n_i = np.array([0.0])
+        T1 = so.transmission(one, vg)
+        t_pot = time.perf_counter() - t0
+        T = np.repeat(T1, sample_slices, axis=0)
+        rows = req.beginrow + (np.arange(workers) // req.width_red) * req.step
+        cols = req.begincol + (np.arange(workers) % req.width_red) * req.step
+        jobs = [(req.probe[0], T, int(rows[i]), int(cols[i]), req.prop) for i in range(workers)]
+        t0 = time.perf_counter()
+        list(ex.map(_loop_sample, jobs))
+        t_loop = time.perf_counter() - t0
+    rate = workers * sample_slices / t_loop
+    total = req.slices * t_pot + req.probe_slices / rate
+    value = req.probe_slices / total
+    sample = (f"oracle (FP64 NumPy/SciPy) on {workers} processes: potential+transmission of 1 of "
+              f"{req.slices} slices ({n0} atoms, {req.p_height}^2 grid) in {t_pot:.2f} s; {workers} probes x "
+              f"{sample_slices} slices ({req.height}^2 window) in {t_loop:.2f} s; extrapolated to "
+              f"{req.probe_slices} probe*slices")
+    return value, sample, t_pot + t_loop
+
+
+# ----------------------------------------------------------------------------------------------
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(ns):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import stem_oracle as so
+    req = build_workload(ns.workload)
+    workers = so.cpu_count()
+    for _ in range(ns.warmup):
+        cpu_sample(req, workers, sample_slices=1)
+    vals, samples, secs = [], None, 0.0
+    for _ in range(ns.steps):
+        v, samples, s = cpu_sample(req, workers)
+        vals.append(v)
+        secs += s
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": "STEM probe*slices/s", "value": value, "unit": "probe*slices/s",
+        "n_gpus": ns.gpus, "steps": ns.steps, "warmup": ns.warmup,
+        "ms_per_step": 1000.0 * secs / max(ns.steps, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SrTiO3 supercell)",
+        "config": workload_config(ns, req),
+        "cpu_baseline": {"value": value, "unit": "probe*slices/s", "cores": workers, "kind": "port",
+                         "sample": samples},
+        "e2e": {"value": value, "unit": "probe*slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(ns, req):
+    return {"workload": f"{ns.workload}: SrTiO3 [001] STEM-ADF, {req.depth} probes x {req.slices} slices, "
+                        f"window {req.height}^2, potential {req.p_height}^2, Peng, 300 kV",
+            "probes": req.depth, "slices": req.slices, "window": req.height, "potential_grid": req.p_height,
+            "detectors": req.aper_num, "path": ns.path, "l2": "inputs larger than L2 (transmission stack "
+            f"{req.slices * req.p_height * req.p_width * 8 / 2**20:.0f} MiB)",
+            "parallelism": f"probe shards, {ns.gpus} GPU(s), no collective in the data path"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="stem-adf")
+    ap.add_argument("--path", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ns = ap.parse_args()
+    if ns.impl == "reference":
+        run_reference(ns)
+        return
+
+    import torch
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    from totem_b200 import capi
+    path = capi.PATH_FUSED if ns.path == "fused" else capi.PATH_PLAIN
+    req = build_workload(ns.workload)
+    stream = torch.cuda.current_stream()
+    sess = capi.Session(device=local, stream=stream.cuda_stream)
+    sess.upload(req)
+
+    def step():
+        sess.run(path=path, batch=ns.batch)
+
+    for _ in range(max(ns.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    launches = sess.timing().kernel_launches
+    batch_used = sess.timing().batch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(ns.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / ns.steps
+    units = req.probe_slices
+    value = ws * units * ns.steps / (ms_total / 1000.0)
+
+    # per-kernel device times (events around every pass) for the roofline
+    sess.run(path=path, batch=ns.batch, profile=True)
+    tm = sess.timing()
+    peak, peak_kind = measured_peaks()
+    n2 = req.height * req.width
+    roofline = None
+    if path == capi.PATH_FUSED and tm.row_pass_launches:
+        alg_bytes = units * 3 * n2 * BYTES_PER_ELEM  # read psi, write psi, read T window
+        step_ms = tm.row_pass_ms + tm.col_pass_ms
+        achieved = alg_bytes / (step_ms / 1000.0) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "slice_step_traffic.json")
+        if os.path.exists(tpath):
+            tr = json.load(open(tpath))
+            if tr.get("window") == req.height:
+                traffic = tr["dram_bytes_per_probe_slice"] * units / tm.col_pass_launches
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic,
+                    "kernel": "slice step = k_row_pass + k_col_pass (one launch of each per slice)",
+                    "algorithmic_bytes_per_probe_slice": 3 * n2 * BYTES_PER_ELEM,
+                    "row_pass_ms_avg": tm.row_pass_ms / tm.row_pass_launches,
+                    "col_pass_ms_avg": tm.col_pass_ms / tm.col_pass_launches,
+                    "probes_per_launch": tm.batch,
+                    "transmission_ms": tm.transmission_ms, "slice_loop_ms": tm.slice_loop_ms}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not ns.no_e2e:
+        capi.stem_run(req, path=path, batch=ns.batch)  # warm the default session
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ns.steps):
+            capi.stem_run(req, path=path, batch=ns.batch)
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        h2d = tm.h2d_bytes
+        d2h = 8 * req.aper_num * req.depth * (1 + len(req.mid_layer))
+        e2e = {"value": ws * units * ns.steps / dt, "unit": "probe*slices/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "api": "totem_stem_run (host buffers)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not ns.no_cpu_baseline:
+        from oracle import stem_oracle as so
+        cores = so.cpu_count()
+        v, sample, _ = cpu_sample(req, cores)
+        cpu = {"value": v, "unit": "probe*slices/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "STEM probe*slices/s", "value": value, "unit": "probe*slices/s", "n_gpus": ws,
+            "steps": ns.steps, "warmup": ns.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (complex64; FP64 detector sums)",
+            "data": "synthetic (seeded SrTiO3 supercell, random-free probe)",
+            "config": workload_config(ns, req), "batch": batch_used,
+            "gpu_launches": launches * ns.steps, "clocks": clk.summary(), "roofline": roofline,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sess.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

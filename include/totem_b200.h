@@ -1,0 +1,181 @@
+/*
+ * totem_b200 -- B200-native multislice STEM engine, C ABI.
+ *
+ * The engine replaces the GPU back end of ToTem's MEX entry points
+ *   waveCudalobato_<v>, waveCudaPengAndCorr_<v>        (STEM: cuda_stem.m:83-106)
+ *   waveCudalobatoP_<v>, waveCudaPengAndCorrP_<v>      (transmission only: cuda_stem_potential.m)
+ * whose MEX shim (waveCuda.cpp:4-101) forwards 41 MATLAB arguments to the C++ function
+ *   void myProjectfun(...)                             (waveCuda.h:10-21)
+ * implemented by cuda_source_lobato.cu:1018-1562 / cuda_source_peng_and_corr.cu:1217-1786 and,
+ * for the transmission-only variants, cuda_source_lobato_potential.cu:747-927 /
+ * cuda_source_peng_and_corr_potential.cu:952-1149.
+ *
+ * Two ways in:
+ *   1. ``myProjectfun`` with the reference's exact 44-parameter C++ signature, exported by the
+ *      four small libraries libwaveCuda{Lobato,Peng,LobatoP,PengP}.so so that the unchanged
+ *      waveCuda.cpp links against them (declared at the end of this header, C++ only).
+ *   2. The C entry points below (plain pointers and sizes, status codes, no torch types).
+ *
+ * Array layouts are the ones ``myProjectfun`` receives: every matrix is row-major with the
+ * MATLAB row index first (the MEX caller transposes, cuda_stem.m:22-58); stacks are
+ * (count, rows, cols).  All arrays passed in are host memory; a session keeps its uploaded
+ * inputs resident on the device between runs.
+ */
+#ifndef TOTEM_B200_H
+#define TOTEM_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define TOTEM_API __attribute__((visibility("default")))
+#else
+#define TOTEM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TOTEM_ABI_VERSION 1
+
+/* Status codes.  The reference returns silently or aborts MATLAB (waveCuda.cpp:7-16,
+ * cuda_source_lobato.cu:1253-1256); every entry point here returns one of these instead. */
+enum {
+  TOTEM_OK = 0,
+  TOTEM_ERR_INVALID_ARG = 1,   /* a size, pointer or index is out of range            */
+  TOTEM_ERR_UNSUPPORTED = 2,   /* valid input this build does not handle (e.g. sizes) */
+  TOTEM_ERR_CUDA = 3,          /* a CUDA runtime call failed                          */
+  TOTEM_ERR_CUFFT = 4,         /* a cuFFT call failed                                 */
+  TOTEM_ERR_OOM = 5,           /* device allocation failed                            */
+  TOTEM_ERR_NO_DEVICE = 6,     /* no CUDA device is visible                           */
+  TOTEM_ERR_STATE = 7          /* call sequence error (e.g. run before upload)        */
+};
+
+/* Scattering-factor parameterisation: selects the coefficient-row layout, i.e. which MEX the
+ * request targets (cuda_stem.m:83-94). */
+enum { TOTEM_PARAM_PENG = 0,   /* rows of 13 (neutral) / 25 (ionic) columns */
+       TOTEM_PARAM_LOBATO = 1  /* rows of 14 / 26 columns                     */ };
+
+/* Slice-loop implementation. */
+enum { TOTEM_PATH_FUSED = 0,   /* shared-memory FFT passes fused with the multiplies and detectors */
+       TOTEM_PATH_PLAIN = 1    /* cuFFT plus separate element-wise kernels (comparator)           */ };
+
+/*
+ * The inputs of myProjectfun (waveCuda.h:10-21), one field per parameter, same meaning.
+ */
+typedef struct TotemStemArgs {
+  int struct_size;                 /* sizeof(TotemStemArgs)                                    */
+  int param;                       /* TOTEM_PARAM_*                                            */
+
+  const double *probe_re, *probe_im; /* w_num x height x width (prhs[0..1])                    */
+  const double *aper;              /* aper_num x height x width, centred masks (prhs[2])       */
+  const double *atom_slice;        /* slices: neutral rows per slice (prhs[3], series_n)       */
+  const double *absorp_n;          /* rows x 10 absorptive coefficients or NULL (prhs[4])      */
+  const double *atom_slice_i;      /* slices: ionic rows per slice (prhs[5])                   */
+  const double *absorp_n_i;        /* or NULL (prhs[6])                                        */
+  const double *proj_coff_mat;     /* neutral rows x 13|14 (prhs[7])                           */
+  const double *proj_coff_mat_i;   /* ionic rows x 25|26 (prhs[8])                             */
+  const double *kx, *ky, *s_2;     /* p_height x p_width (prhs[9..11])                         */
+  const double *prop_re, *prop_im; /* height x width Fresnel propagator, FFT order (prhs[12..13]) */
+  const double *gfsf;              /* w_num weights (prhs[14])                                 */
+  int height, width, depth;        /* window rows, cols; scan positions (prhs[15..17])         */
+  int p_height, p_width, slices;   /* potential grid and slice count (prhs[18..20])            */
+  int step;                        /* scan step in pixels (prhs[21])                           */
+  int begin_row, begin_col;        /* 0-based window origin (prhs[22..23] minus one)           */
+  int width_red;                   /* scan positions per scan row (prhs[24])                   */
+  double sigma;                    /* interaction constant, 1/(kV*A) (prhs[25])               */
+  int w_num, aper_num;             /* probes (defocus spread) and detectors (prhs[26..27])     */
+  double parameter;                /* PARAMETER (prhs[28])                                     */
+  const double *aper_true;         /* p_height x p_width multiplier of V(g) (prhs[29])         */
+  const int *mid_layer;            /* 1-based slice indices (prhs[32])                         */
+  int layer_len;                   /* (prhs[33])                                               */
+  const double *aper2;             /* aper_num x height x width, ifftshift(aper) (prhs[34])    */
+  const double *series_n_corr;     /* slices or NULL (prhs[35])                                */
+  const double *series_n_i_corr;   /* slices or NULL (prhs[36])                                */
+  const double *ele_n_corr;        /* rows x 5 (prhs[37])                                      */
+  const double *ele_n_i_corr;      /* rows x 8 (prhs[38])                                      */
+  const double *corr_info_matrix;  /* cim_len x p_height x p_width (prhs[39])                  */
+  int cim_len;                     /* (prhs[40])                                               */
+} TotemStemArgs;
+
+/* Outputs (plhs[0..3] of waveCuda.cpp:85-92).  NULL pointers are skipped. */
+typedef struct TotemStemOut {
+  double *result;                  /* aper_num*depth, result[a*depth + pos]                    */
+  double *mid_layer_mat;           /* depth*aper_num*layer_len, [(l*aper_num + a)*depth + pos]  */
+  double *potential_re;            /* p_height*p_width*slices, transmission (the *P variants)  */
+  double *potential_im;
+} TotemStemOut;
+
+/* Engine options of one run (defaults: all zero). */
+typedef struct TotemRunOptions {
+  int path;                        /* TOTEM_PATH_*                                              */
+  int batch;                       /* probes in flight per batch, 0 = engine's choice          */
+  int skip_transmission;           /* 1 = reuse the transmission built by an earlier run        */
+  int profile;                     /* 1 = CUDA events around every slice-loop pass launch       */
+} TotemRunOptions;
+
+/* Device times (CUDA events) of the last run, milliseconds. */
+typedef struct TotemTiming {
+  float transmission_ms;
+  float slice_loop_ms;
+  float total_ms;
+  int kernel_launches;             /* kernels this engine launched in the run                  */
+  int batch;                       /* batch size used                                          */
+  /* profile = 1 only: summed device time and launch count of the fused passes */
+  float row_pass_ms, col_pass_ms;
+  int row_pass_launches, col_pass_launches;
+  long long probe_slices;          /* probes x slices advanced by the run                      */
+  long long h2d_bytes, d2h_bytes;  /* host<->device bytes of the last upload / download        */
+} TotemTiming;
+
+typedef struct totem_session totem_session;
+
+TOTEM_API int totem_abi_version(void);
+TOTEM_API const char *totem_status_string(int status);
+/* Message describing the last failure on the calling thread ("" if none). */
+TOTEM_API const char *totem_last_error(void);
+
+/* A session owns device buffers on one GPU and keeps them between calls.  ``device`` = -1
+ * selects the GPU with the most free memory, as the reference does
+ * (cuda_source_lobato.cu:1071-1081).  ``stream`` is a cudaStream_t (NULL = the session makes one). */
+TOTEM_API int totem_session_create(int device, void *stream, totem_session **out);
+TOTEM_API int totem_session_destroy(totem_session *s);
+/* Copy (or, for TOTEM_MEM_DEVICE, adopt) the request's inputs and validate them. */
+TOTEM_API int totem_session_upload(totem_session *s, const TotemStemArgs *args);
+/* Device work only: transmission build, slice loop, detector reduction.  Results stay on the
+ * device.  ``what`` = 0: STEM; 1: transmission only.  Asynchronous on the session's stream. */
+TOTEM_API int totem_session_run(totem_session *s, int what, const TotemRunOptions *opt);
+/* Wait for the stream and copy results into ``out`` (host pointers). */
+TOTEM_API int totem_session_download(totem_session *s, TotemStemOut *out);
+TOTEM_API int totem_session_timing(totem_session *s, TotemTiming *t);
+/* Device pointer of the transmission stack (complex64, slices x p_height x p_width). */
+TOTEM_API int totem_session_transmission(totem_session *s, void **ptr);
+
+/* One call with host buffers: the semantics of the STEM MEX (result, mid_layer_mat).
+ * Replaces myProjectfun in cuda_source_lobato.cu:1018 / cuda_source_peng_and_corr.cu:1217. */
+TOTEM_API int totem_stem_run(const TotemStemArgs *args, const TotemRunOptions *opt, TotemStemOut *out);
+/* One call with host buffers: the semantics of the *P MEX (potential_re/im = Re/Im of the
+ * transmission exp(i sigma V / 1000)).  Replaces cuda_source_lobato_potential.cu:747. */
+TOTEM_API int totem_transmission_run(const TotemStemArgs *args, TotemStemOut *out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+
+/* The reference's own entry point, C++ linkage, exact signature of waveCuda.h:10-21.
+ * Exported by libwaveCudaLobato.so / libwaveCudaPeng.so (STEM) and libwaveCudaLobatoP.so /
+ * libwaveCudaPengP.so (transmission only). */
+TOTEM_API void myProjectfun(double *my_real_w, double *my_imag_w, double *aper,
+                  double *atom_slice, double *absorp_n, double *atom_slice_i,
+                  double *absorp_n_i, double *proj_coff_mat, double *proj_coff_mat_i,
+                  double *kx, double *ky, double *s_2, double *my_real_const,
+                  double *my_img_const, double *gfsf, int Height, int Width, int Depth,
+                  int P_Height, int P_Width, int Slices, int step, int beginRow, int beginCol,
+                  int width_red, double sigma, int w_num, int aper_num, double parameter,
+                  double *AperTrue, int *mid_ceng, int ceng_len, double *aper2,
+                  double *series_n_corr, double *series_n_i_corr,
+                  double *ele_n_corr, double *ele_n_i_corr,
+                  double *corr_info_matrix, int cim_len,
+                  double *return_result, double *mid_ceng_mat, double *potentialx, double *potentialy);
+#endif
+
+#endif /* TOTEM_B200_H */

@@ -1,0 +1,124 @@
+"""CUDA engine vs the FP64 oracle, through the C ABI (``totem_stem_run`` / sessions /
+``myProjectfun``).
+
+Tolerance: relative L2 <= 1e-4 on every detector image and on the transmission stack -- the
+accuracy target of the FP32 engine against FP64.
+"""
+import numpy as np
+import pytest
+
+from oracle import stem_oracle as so
+from tests.conftest import rel_l2
+from totem_b200 import capi, request
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def _check(req, res, mid, tol=TOL):
+    T = so.transmission(req)
+    ref_res, ref_mid = so.stem(req, T)
+    A, D, L = req.aper_num, req.depth, len(req.mid_layer)
+    r, rr = res.reshape(A, D), ref_res.reshape(A, D)
+    for a in range(A):
+        assert rel_l2(r[a], rr[a]) < tol, (a, rel_l2(r[a], rr[a]))
+    if L:
+        m, rm = mid.reshape(L, A, D), ref_mid.reshape(L, A, D)
+        for l in range(L):
+            for a in range(A):
+                if np.linalg.norm(rm[l, a]) == 0:
+                    assert np.all(m[l, a] == 0)
+                else:
+                    assert rel_l2(m[l, a], rm[l, a]) < tol, (l, a, rel_l2(m[l, a], rm[l, a]))
+
+
+@pytest.mark.parametrize("flag", ["p", "l"])
+@pytest.mark.parametrize("path", [capi.PATH_FUSED, capi.PATH_PLAIN])
+def test_stem_small_vs_oracle(engine_lib, flag, path):
+    req = request.build_small_stem(flag=flag)
+    res, mid = capi.stem_run(req, path=path)
+    _check(req, res, mid)
+
+
+@pytest.mark.parametrize("n,p", [(128, 256), (256, 512)])
+def test_stem_window_sizes(engine_lib, n, p):
+    req = request.build_small_stem(n=n, p=p, raster=(2, 2), step=17, slices=4, sampling=0.1, mid_layer=(1, 4))
+    res, mid = capi.stem_run(req)
+    _check(req, res, mid)
+
+
+def test_transmission_vs_oracle(engine_lib):
+    req = request.build_small_stem(flag="l")
+    t = capi.transmission_run(req)
+    ref = so.transmission(req)
+    assert rel_l2(t, ref) < TOL
+    # the *P MEX flavour through the reference's own entry-point signature
+    t2 = capi.call_myprojectfun(req, transmission=True)
+    assert rel_l2(t2, ref) < TOL
+
+
+def test_myprojectfun_stem_abi(engine_lib):
+    req = request.build_small_stem(flag="p", mid_layer=(3,))
+    res, mid = capi.call_myprojectfun(req, transmission=False)
+    _check(req, res, mid)
+
+
+def test_defocus_spread_and_unsorted_layers(engine_lib):
+    # w_num > 1 with gfsf weights; mid layers unsorted, repeated and out of range
+    req = request.build_small_stem(focal_steps=3, mid_layer=(5, 2, 5, 99, 6))
+    res, mid = capi.stem_run(req)
+    _check(req, res, mid)
+
+
+def test_absorptive_and_ionic_rows(engine_lib):
+    from totem_b200 import specimen
+    req = request.build_small_stem(flag="p")
+    # turn a third of the atoms into partly ionic O (O2-), plus absorptive rows on everything
+    rows = req.ele_n
+    n = len(rows)
+    ion_idx = np.arange(0, n, 3)
+    o2 = specimen.ion_params(8, -2)
+    neutral_o = specimen.element_params(8, "p")
+    ion_rows = np.zeros((len(ion_idx), 25))
+    ion_rows[:, 0:3] = rows[ion_idx, 0:3]
+    ion_rows[:, 3] = 0.4
+    ion_rows[:, 4:14:2], ion_rows[:, 5:14:2] = o2[:5], o2[5:]
+    ion_rows[:, 14] = 0.6
+    ion_rows[:, 15:25:2], ion_rows[:, 16:25:2] = neutral_o[:5], neutral_o[5:]
+    keep = np.setdiff1d(np.arange(n), ion_idx)
+    # per-slice counts of both kinds
+    beg = np.concatenate([[0], np.cumsum(req.series_n)]).astype(int)
+    sl = np.searchsorted(beg, np.arange(n), side="right") - 1
+    series_n = np.bincount(sl[keep], minlength=req.slices).astype(float)
+    series_i = np.bincount(sl[ion_idx], minlength=req.slices).astype(float)
+    from dataclasses import replace
+    req2 = replace(req, ele_n=rows[keep], series_n=series_n, ele_n_i=ion_rows, series_n_i=series_i)
+    req2 = request.with_absorption(req2)
+    res, mid = capi.stem_run(req2)
+    _check(req2, res, mid)
+
+
+def test_session_reuse_and_batches(engine_lib):
+    req = request.build_small_stem(raster=(4, 5))
+    s = capi.Session()
+    s.upload(req)
+    outs = []
+    for b in (1, 3, 7, 0):
+        s.run(batch=b)
+        res, mid, _ = s.download()
+        outs.append((res, mid))
+    for r, m in outs[1:]:
+        assert np.array_equal(r, outs[0][0]) and np.array_equal(m, outs[0][1])  # batch-composition invariance
+    _check(req, *outs[0])
+    t = s.timing()
+    assert t.kernel_launches > 0 and t.total_ms > 0
+    s.close()
+
+
+def test_invalid_window_rejected(engine_lib):
+    req = request.build_small_stem()
+    from dataclasses import replace
+    bad = replace(req, begincol=req.p_width - req.width + 1)
+    with pytest.raises(capi.TotemError) as e:
+        capi.stem_run(bad)
+    assert e.value.code == capi.ERR_INVALID_ARG

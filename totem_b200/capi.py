@@ -1,0 +1,302 @@
+"""ctypes binding of ``include/totem_b200.h`` (the engine's C ABI).
+
+Loading fails loudly when the shared library is missing: there is no CPU or PyTorch fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+CORE_PATH = os.path.join(LIB_DIR, "libtotem_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "totem_b200.h")
+SHIM_LIBS = {("p", False): "libwaveCudaPeng.so", ("l", False): "libwaveCudaLobato.so",
+             ("p", True): "libwaveCudaPengP.so", ("l", True): "libwaveCudaLobatoP.so"}
+
+OK, ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_CUFFT, ERR_OOM, ERR_NO_DEVICE, ERR_STATE = range(8)
+PARAM_PENG, PARAM_LOBATO = 0, 1
+PATH_FUSED, PATH_PLAIN = 0, 1
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class TotemStemArgs(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int), ("param", C.c_int),
+        ("probe_re", _dp), ("probe_im", _dp), ("aper", _dp),
+        ("atom_slice", _dp), ("absorp_n", _dp), ("atom_slice_i", _dp), ("absorp_n_i", _dp),
+        ("proj_coff_mat", _dp), ("proj_coff_mat_i", _dp),
+        ("kx", _dp), ("ky", _dp), ("s_2", _dp), ("prop_re", _dp), ("prop_im", _dp), ("gfsf", _dp),
+        ("height", C.c_int), ("width", C.c_int), ("depth", C.c_int),
+        ("p_height", C.c_int), ("p_width", C.c_int), ("slices", C.c_int), ("step", C.c_int),
+        ("begin_row", C.c_int), ("begin_col", C.c_int), ("width_red", C.c_int),
+        ("sigma", C.c_double), ("w_num", C.c_int), ("aper_num", C.c_int), ("parameter", C.c_double),
+        ("aper_true", _dp), ("mid_layer", _ip), ("layer_len", C.c_int), ("aper2", _dp),
+        ("series_n_corr", _dp), ("series_n_i_corr", _dp), ("ele_n_corr", _dp), ("ele_n_i_corr", _dp),
+        ("corr_info_matrix", _dp), ("cim_len", C.c_int),
+    ]
+
+
+class TotemStemOut(C.Structure):
+    _fields_ = [("result", _dp), ("mid_layer_mat", _dp), ("potential_re", _dp), ("potential_im", _dp)]
+
+
+class TotemRunOptions(C.Structure):
+    _fields_ = [("path", C.c_int), ("batch", C.c_int), ("skip_transmission", C.c_int), ("profile", C.c_int)]
+
+
+class TotemTiming(C.Structure):
+    _fields_ = [("transmission_ms", C.c_float), ("slice_loop_ms", C.c_float), ("total_ms", C.c_float),
+                ("kernel_launches", C.c_int), ("batch", C.c_int),
+                ("row_pass_ms", C.c_float), ("col_pass_ms", C.c_float),
+                ("row_pass_launches", C.c_int), ("col_pass_launches", C.c_int),
+                ("probe_slices", C.c_longlong), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong)]
+
+
+class TotemError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"totem_b200 error {code}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+
+def library_path() -> str:
+    return CORE_PATH
+
+
+def load() -> C.CDLL:
+    """Load ``libtotem_b200.so`` (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(CORE_PATH):
+        raise RuntimeError(f"{CORE_PATH} is missing: run `python -m totem_b200.build` "
+                           "(this engine has no CPU fallback)")
+    lib = C.CDLL(CORE_PATH)
+    vp = C.c_void_p
+    lib.totem_abi_version.restype = C.c_int
+    lib.totem_status_string.restype = C.c_char_p
+    lib.totem_status_string.argtypes = [C.c_int]
+    lib.totem_last_error.restype = C.c_char_p
+    lib.totem_session_create.argtypes = [C.c_int, vp, C.POINTER(vp)]
+    lib.totem_session_destroy.argtypes = [vp]
+    lib.totem_session_upload.argtypes = [vp, C.POINTER(TotemStemArgs)]
+    lib.totem_session_run.argtypes = [vp, C.c_int, C.POINTER(TotemRunOptions)]
+    lib.totem_session_download.argtypes = [vp, C.POINTER(TotemStemOut)]
+    lib.totem_session_timing.argtypes = [vp, C.POINTER(TotemTiming)]
+    lib.totem_session_transmission.argtypes = [vp, C.POINTER(vp)]
+    lib.totem_stem_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemRunOptions), C.POINTER(TotemStemOut)]
+    lib.totem_transmission_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemStemOut)]
+    for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
+                 "totem_session_download", "totem_session_timing", "totem_session_transmission",
+                 "totem_stem_run", "totem_transmission_run"):
+        getattr(lib, name).restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+def check(rc: int):
+    if rc != OK:
+        lib = load()
+        raise TotemError(rc, f"{lib.totem_status_string(rc).decode()}: {lib.totem_last_error().decode()}")
+
+
+def header_functions() -> list[str]:
+    """Names of the C functions declared in ``include/totem_b200.h``."""
+    text = open(HEADER).read()
+    c_part = text.split("#ifdef __cplusplus\n} /* extern \"C\" */")[0]
+    return sorted(set(re.findall(r"\b(totem_[a-z_]+)\s*\(", c_part)))
+
+
+# ----------------------------------------------------------------------------------------------
+# numpy <-> struct marshalling
+# ----------------------------------------------------------------------------------------------
+
+def _d(a):
+    if a is None:
+        return None
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a, typ=_dp):
+    if a is None:
+        return C.cast(None, typ)
+    return a.ctypes.data_as(typ)
+
+
+class Marshalled:
+    """Keeps the numpy buffers referenced by a TotemStemArgs alive."""
+
+    def __init__(self, req, stem: bool = True):
+        self.keep = []
+
+        def k(a):
+            a = _d(a)
+            if a is not None:
+                self.keep.append(a)
+            return a
+        series_n, series_n_i = req.padded_series()
+        a = TotemStemArgs()
+        a.struct_size = C.sizeof(TotemStemArgs)
+        a.param = PARAM_LOBATO if req.param == "l" else PARAM_PENG
+        if stem:
+            a.probe_re = _ptr(k(req.probe.real))
+            a.probe_im = _ptr(k(req.probe.imag))
+            a.aper = _ptr(k(req.aper))
+            a.prop_re = _ptr(k(req.prop.real))
+            a.prop_im = _ptr(k(req.prop.imag))
+            a.gfsf = _ptr(k(req.gfsf))
+            a.aper2 = _ptr(k(req.aper2))
+            a.height, a.width = req.height, req.width
+            a.depth = req.depth
+            a.step, a.begin_row, a.begin_col, a.width_red = req.step, req.beginrow, req.begincol, req.width_red
+            a.w_num, a.aper_num = req.w_num, req.aper_num
+            mid = np.ascontiguousarray(req.mid_layer, dtype=np.int32)
+            self.keep.append(mid)
+            a.mid_layer = mid.ctypes.data_as(_ip)
+            a.layer_len = len(mid)
+        else:
+            a.w_num = 1
+        a.atom_slice = _ptr(k(series_n))
+        a.atom_slice_i = _ptr(k(series_n_i))
+        a.absorp_n = _ptr(k(req.absorp_n))
+        a.absorp_n_i = _ptr(k(req.absorp_n_i))
+        a.proj_coff_mat = _ptr(k(req.ele_n if len(req.ele_n) else None))
+        a.proj_coff_mat_i = _ptr(k(req.ele_n_i if len(req.ele_n_i) else None))
+        a.kx, a.ky, a.s_2 = _ptr(k(req.kx)), _ptr(k(req.ky)), _ptr(k(req.s2))
+        a.p_height, a.p_width, a.slices = req.p_height, req.p_width, req.slices
+        a.sigma, a.parameter = req.sigma, req.parameter
+        a.aper_true = _ptr(k(req.aper_true))
+        if req.corr_info_matrix is not None and len(req.corr_info_matrix):
+            a.series_n_corr = _ptr(k(req.series_n_corr))
+            a.series_n_i_corr = _ptr(k(req.series_n_i_corr))
+            a.ele_n_corr = _ptr(k(req.ele_n_corr))
+            a.ele_n_i_corr = _ptr(k(req.ele_n_i_corr))
+            a.corr_info_matrix = _ptr(k(req.corr_info_matrix))
+            a.cim_len = len(req.corr_info_matrix)
+        self.args = a
+
+
+class Session:
+    """A device session: inputs uploaded once, runs on the device, results fetched on demand."""
+
+    def __init__(self, device: int = -1, stream: int | None = None):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.totem_session_create(device, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+        self.req = None
+        self._m = None
+
+    def close(self):
+        if self.h:
+            self.lib.totem_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, req, stem: bool = True):
+        self._m = Marshalled(req, stem)
+        self.req = req
+        check(self.lib.totem_session_upload(self.h, C.byref(self._m.args)))
+
+    def run(self, what: int = 0, path: int = PATH_FUSED, batch: int = 0, skip_transmission: bool = False,
+            profile: bool = False):
+        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile))
+        check(self.lib.totem_session_run(self.h, what, C.byref(o)))
+
+    def download(self, want_transmission: bool = False):
+        req = self.req
+        out = TotemStemOut()
+        res = mid = tre = tim = None
+        if req.depth:
+            res = np.zeros(req.aper_num * req.depth)
+            mid = np.zeros(req.aper_num * req.depth * len(req.mid_layer))
+            out.result = _ptr(res)
+            out.mid_layer_mat = _ptr(mid)
+        if want_transmission:
+            n = req.p_height * req.p_width * req.slices
+            tre, tim = np.zeros(n), np.zeros(n)
+            out.potential_re, out.potential_im = _ptr(tre), _ptr(tim)
+        check(self.lib.totem_session_download(self.h, C.byref(out)))
+        t = None
+        if want_transmission:
+            t = (tre + 1j * tim).reshape(req.slices, req.p_height, req.p_width)
+        return res, mid, t
+
+    def timing(self) -> TotemTiming:
+        t = TotemTiming()
+        check(self.lib.totem_session_timing(self.h, C.byref(t)))
+        return t
+
+
+def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
+    """One-shot STEM call through ``totem_stem_run`` (host buffers in, host buffers out)."""
+    lib = load()
+    m = Marshalled(req, True)
+    res = np.zeros(req.aper_num * req.depth)
+    mid = np.zeros(req.aper_num * req.depth * len(req.mid_layer))
+    out = TotemStemOut(_ptr(res), _ptr(mid), None, None)
+    opt = TotemRunOptions(path, batch, 0, 0)
+    check(lib.totem_stem_run(C.byref(m.args), C.byref(opt), C.byref(out)))
+    return res, mid
+
+
+def transmission_run(req):
+    """One-shot transmission (the ``*P`` MEX semantics) through ``totem_transmission_run``."""
+    lib = load()
+    m = Marshalled(req, False)
+    n = req.p_height * req.p_width * req.slices
+    tre, tim = np.zeros(n), np.zeros(n)
+    out = TotemStemOut(None, None, _ptr(tre), _ptr(tim))
+    check(lib.totem_transmission_run(C.byref(m.args), C.byref(out)))
+    return (tre + 1j * tim).reshape(req.slices, req.p_height, req.p_width)
+
+
+# ----------------------------------------------------------------------------------------------
+# The reference's own entry point: myProjectfun (C++ linkage) from the MEX-flavour libraries
+# ----------------------------------------------------------------------------------------------
+
+MYPROJECTFUN_MANGLED = ("_Z12myProjectfunPdS_S_S_S_S_S_S_S_S_S_S_S_S_S_iiiiiiiiiidiidS_PiiS_S_S_S_S_S_iS_S_S_S_")
+
+
+def myprojectfun_lib(param: str, transmission: bool) -> C.CDLL:
+    load()  # the core library must be loadable first (the shims link against it)
+    path = os.path.join(LIB_DIR, SHIM_LIBS[(param, transmission)])
+    lib = C.CDLL(path)
+    f = getattr(lib, MYPROJECTFUN_MANGLED)
+    f.restype = None
+    f.argtypes = [_dp] * 15 + [C.c_int] * 10 + [C.c_double, C.c_int, C.c_int, C.c_double, _dp, _ip, C.c_int,
+                                                _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+    return lib
+
+
+def call_myprojectfun(req, transmission: bool = False):
+    """Call ``myProjectfun`` exactly as waveCuda.cpp does (beginRow/beginCol already 0-based)."""
+    lib = myprojectfun_lib(req.param, transmission)
+    f = getattr(lib, MYPROJECTFUN_MANGLED)
+    m = Marshalled(req, not transmission)
+    a = m.args
+    res = np.zeros(max(1, req.aper_num * req.depth))
+    mid = np.zeros(max(1, req.aper_num * req.depth * len(req.mid_layer)))
+    n = req.p_height * req.p_width * req.slices
+    px, py = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+    f(a.probe_re, a.probe_im, a.aper, a.atom_slice, a.absorp_n, a.atom_slice_i, a.absorp_n_i, a.proj_coff_mat,
+      a.proj_coff_mat_i, a.kx, a.ky, a.s_2, a.prop_re, a.prop_im, a.gfsf, a.height, a.width, a.depth, a.p_height,
+      a.p_width, a.slices, a.step, a.begin_row, a.begin_col, a.width_red, a.sigma, a.w_num, a.aper_num,
+      a.parameter, a.aper_true, a.mid_layer, a.layer_len, a.aper2, a.series_n_corr, a.series_n_i_corr,
+      a.ele_n_corr, a.ele_n_i_corr, a.corr_info_matrix, a.cim_len, _ptr(res), _ptr(mid), _ptr(px), _ptr(py))
+    if transmission:
+        return (px[:n] + 1j * py[:n]).reshape(req.slices, req.p_height, req.p_width)
+    return res[: req.aper_num * req.depth], mid[: req.aper_num * req.depth * len(req.mid_layer)]

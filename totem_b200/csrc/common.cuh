@@ -1,0 +1,140 @@
+// Shared declarations of the engine's device code and its host-side launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <cstdint>
+#include <string>
+
+#include "../../include/totem_b200.h"
+
+namespace totem {
+
+// Host-side status carrier used across the engine's C++ code.
+struct Status {
+  int code = TOTEM_OK;
+  std::string msg;
+  bool ok() const { return code == TOTEM_OK; }
+  static Status Ok() { return Status(); }
+  static Status Err(int c, std::string m) {
+    Status s;
+    s.code = c;
+    s.msg = std::move(m);
+    return s;
+  }
+};
+
+Status cuda_status(cudaError_t e, const char* what);
+Status cufft_status(cufftResult r, const char* what);
+// Raise a kernel's dynamic shared-memory limit once (cached per function pointer).
+Status ensure_smem(const void* func, size_t bytes);
+
+#define TOTEM_CUDA(call)                                              \
+  do {                                                                \
+    cudaError_t _e = (call);                                          \
+    if (_e != cudaSuccess) return ::totem::cuda_status(_e, #call);    \
+  } while (0)
+#define TOTEM_CUFFT(call)                                             \
+  do {                                                                \
+    cufftResult _r = (call);                                          \
+    if (_r != CUFFT_SUCCESS) return ::totem::cufft_status(_r, #call); \
+  } while (0)
+#define TOTEM_TRY(expr)                    \
+  do {                                     \
+    ::totem::Status _s = (expr);           \
+    if (!_s.ok()) return _s;               \
+  } while (0)
+
+// Window placement of scan position ``pos``: row offset begin_row + (pos / width_red) * step,
+// column offset begin_col + (pos % width_red) * step (cuda_source_lobato.cu:344-345).
+struct ScanGeom {
+  int begin_row, begin_col, step, width_red, depth, p_width;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Transmission builder
+// ---------------------------------------------------------------------------------------------
+struct AtomRowsDev {
+  const double* pos = nullptr;     // [n][2] x, y in Angstrom (FP64: used for the phase)
+  const float* coef = nullptr;     // [n][ncoef]: the row without x, y (occ, a1, b1, ...)
+  const float* absorp = nullptr;   // [n][10] or null
+  const int* beg = nullptr;        // [slices + 1] first row of every slice
+  int ncoef = 0;
+};
+
+struct TxGrid {
+  int p_h = 0, p_w = 0, slices = 0;
+  int separable = 0;               // kx depends on the column only, ky on the row only
+  const double* kx_axis = nullptr; // [p_w]  (separable)
+  const double* ky_axis = nullptr; // [p_h]
+  const double* kx = nullptr;      // [p_h*p_w] (general)
+  const double* ky = nullptr;
+  const float* s2 = nullptr;       // [p_h*p_w]
+  const float* aper_true = nullptr;// [p_h*p_w] or null (all ones)
+  float parameter = 0.f;
+  int lobato = 0;
+  const float* cim = nullptr;      // [cim_len][p_h*p_w] correction planes or null
+  int cim_len = 0;
+};
+
+// V_k(g) * PARAMETER * APERTURE for all slices into out[slice][p_h][p_w] (complex64).
+Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const AtomRowsDev& ion,
+                           const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out,
+                           cudaStream_t st);
+// In-place unnormalised inverse 2-D FFT of every slice, times (-1)^(r+c) (the ifftshift of the
+// input), then T = exp(i * sigma_scaled * V).  Powers of two only; returns
+// TOTEM_ERR_UNSUPPORTED otherwise.
+Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sigma_scaled,
+                         const float2* tw_w, const float2* tw_h, cudaStream_t st);
+// Element-wise (-1)^(r+c) and exp for the cuFFT builder.
+Status launch_sign_exp(float2* data, long total, int p_h, int p_w, float sigma_scaled, cudaStream_t st);
+
+bool fused_fft_size_ok(int n);
+
+// ---------------------------------------------------------------------------------------------
+// Fused multislice
+// ---------------------------------------------------------------------------------------------
+struct SliceLoopArgs {
+  int n = 0;                       // window edge N (power of two)
+  int items = 0;                   // items in this batch
+  int item0 = 0;                   // first global item (w-major: item = w * depth + pos)
+  ScanGeom geo{};
+  int p_h = 0;
+  float2* psi = nullptr;           // [items][N][N]
+  const float2* probe = nullptr;   // [w_num][N][N]
+  const float2* prop = nullptr;    // [N][N]
+  const float2* tw = nullptr;      // N twiddles
+  int aper_num = 0;
+  const float* mask_mid = nullptr; // [A][N][N] (natural FFT order)
+  const float* mask_exit = nullptr;
+  double* part_mid = nullptr;      // [items][A][nblk]
+  double* part_exit = nullptr;
+};
+int col_blocks(int n);             // number of column blocks per item (partials per detector)
+Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st);
+// flags: 1 = mid-slice detectors, 2 = exit detectors, 4 = final pass (no inverse transform)
+Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st);
+// Sum the per-column-block partials in a fixed order: acc[(w*A + a)*depth + pos].
+Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth,
+                         double* acc, cudaStream_t st);
+// out[i] = sum_w gfsf[w] * acc[w*AD + i], w in ascending order (accumulate_result).
+Status launch_combine(const double* acc, const double* gfsf, int w_num, long ad, double* out, cudaStream_t st);
+
+// ---------------------------------------------------------------------------------------------
+// Plain path (cuFFT + element-wise kernels)
+// ---------------------------------------------------------------------------------------------
+Status launch_plain_init(float2* psi, const float2* probe, int h, int w, int items, int item0, int depth,
+                         cudaStream_t st);
+Status launch_plain_gather_mul(float2* psi, const float2* tslice, int h, int w, int items, int item0,
+                               ScanGeom geo, cudaStream_t st);
+Status launch_plain_mul(float2* psi, const float2* m, int vol, int items, cudaStream_t st);
+Status launch_plain_scale(float2* psi, float s, long total, cudaStream_t st);
+Status launch_plain_detect(const float2* psi, const float* masks, int aper_num, int vol, int items,
+                           double* part, int nblk, cudaStream_t st);
+
+// Conversions used by the uploader.
+Status launch_d2f2(const double* re, const double* im, float2* out, long n, cudaStream_t st);
+Status launch_d2f(const double* in, float* out, long n, cudaStream_t st);
+Status launch_shift_masks(const double* aper, float* out, int aper_num, int h, int w, int shift,
+                          cudaStream_t st);
+
+}  // namespace totem

@@ -1,0 +1,833 @@
+// Engine runtime: sessions, request validation and upload, orchestration of the transmission
+// builder and the slice loop, and the C ABI declared in include/totem_b200.h.
+//
+// Reference orchestrator: myProjectfun (cuda_source_lobato.cu:1018-1562,
+// cuda_source_peng_and_corr.cu:1217-1786).  Differences by design:
+//  * device buffers live in a session and are reused across calls (the reference allocates and
+//    frees everything per call, several buffers per slice);
+//  * no host synchronisation inside the loop, cuFFT plans are created once and cached;
+//  * probes run in batches sized for the L2 cache instead of for half the free memory
+//    (cuda_source_lobato.cu:1250);
+//  * every CUDA / cuFFT status is checked and returned as a TOTEM_ERR_* code.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+using totem::Status;
+
+namespace {
+
+thread_local std::string g_last_error;
+thread_local long long g_h2d_bytes = 0;  // bytes copied host -> device by the current upload
+
+int fail(const Status& s) {
+  g_last_error = s.msg;
+  return s.code;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+  Status ensure(size_t bytes) {
+    if (bytes == 0) bytes = 256;
+    if (bytes <= cap) return Status::Ok();
+    if (p) {
+      cudaFree(p);
+      p = nullptr;
+      cap = 0;
+    }
+    TOTEM_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
+    return Status::Ok();
+  }
+};
+
+template <class T>
+Status upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+  TOTEM_TRY(b.ensure(v.size() * sizeof(T)));
+  if (!v.empty()) TOTEM_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  g_h2d_bytes += (long long)(v.size() * sizeof(T));
+  return Status::Ok();
+}
+
+std::vector<float2> twiddles(int n) {
+  std::vector<float2> t(n);
+  for (int e = 0; e < n; ++e) {
+    const double a = -2.0 * M_PI * (double)e / (double)n;
+    t[e] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  return t;
+}
+
+// Atom rows of one kind, split into FP64 positions and FP32 coefficients.
+struct RowsHost {
+  std::vector<double> pos;
+  std::vector<float> coef;
+  std::vector<float> absorp;
+  std::vector<int> beg;
+  int ncoef = 0;
+  int count = 0;
+};
+
+struct RowsDev {
+  DevBuf pos, coef, absorp, beg;
+  totem::AtomRowsDev view(bool present, bool has_absorp, int ncoef) const {
+    totem::AtomRowsDev d;
+    if (!present) return d;
+    d.pos = pos.as<double>();
+    d.coef = coef.as<float>();
+    d.absorp = has_absorp ? absorp.as<float>() : nullptr;
+    d.beg = beg.as<int>();
+    d.ncoef = ncoef;
+    return d;
+  }
+  Status put(const RowsHost& h, cudaStream_t st) {
+    TOTEM_TRY(upload(pos, h.pos, st));
+    TOTEM_TRY(upload(coef, h.coef, st));
+    TOTEM_TRY(upload(absorp, h.absorp, st));
+    TOTEM_TRY(upload(beg, h.beg, st));
+    return Status::Ok();
+  }
+};
+
+// Per-slice counts -> prefix offsets; validates that the counts are whole, non-negative numbers.
+Status offsets(const double* counts, int slices, std::vector<int>& beg, int& total, const char* what) {
+  beg.assign(slices + 1, 0);
+  total = 0;
+  for (int s = 0; s < slices; ++s) {
+    const double c = counts ? counts[s] : 0.0;
+    if (!(c >= 0.0) || c != std::floor(c) || c > 1e9)
+      return Status::Err(TOTEM_ERR_INVALID_ARG, std::string(what) + ": per-slice count is not a whole number >= 0");
+    total += (int)c;
+    beg[s + 1] = total;
+  }
+  return Status::Ok();
+}
+
+RowsHost split_rows(const double* rows, int count, int ncol, const double* absorp, const std::vector<int>& beg) {
+  RowsHost h;
+  h.count = count;
+  h.ncoef = ncol - 2;
+  h.beg = beg;
+  h.pos.resize((size_t)count * 2);
+  h.coef.resize((size_t)count * h.ncoef);
+  for (int a = 0; a < count; ++a) {
+    h.pos[2 * a] = rows[(size_t)a * ncol];
+    h.pos[2 * a + 1] = rows[(size_t)a * ncol + 1];
+    for (int k = 0; k < h.ncoef; ++k) h.coef[(size_t)a * h.ncoef + k] = (float)rows[(size_t)a * ncol + 2 + k];
+  }
+  if (absorp) {
+    h.absorp.resize((size_t)count * 10);
+    for (size_t i = 0; i < h.absorp.size(); ++i) h.absorp[i] = (float)absorp[i];
+  }
+  return h;
+}
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+struct PlanKey {
+  int h, w, batch;
+  bool operator<(const PlanKey& o) const {
+    return h != o.h ? h < o.h : (w != o.w ? w < o.w : batch < o.batch);
+  }
+};
+
+}  // namespace
+
+struct totem_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::mutex mu;
+
+  // request metadata
+  bool uploaded = false;
+  bool stem_ready = false;  // STEM inputs present (the transmission-only MEX passes none)
+  int param = 0, h = 0, w = 0, depth = 0, p_h = 0, p_w = 0, slices = 0, step = 0, begin_row = 0, begin_col = 0,
+      width_red = 0, w_num = 0, aper_num = 0;
+  double sigma = 0, parameter = 0;
+  std::vector<int> mid_layer;
+  std::vector<double> gfsf;
+  bool separable = false, aper_true_ones = true, has_abs_n = false, has_abs_i = false;
+  int n_rows = 0, n_rows_i = 0, n_corr = 0, n_corr_i = 0, cim_len = 0, ncoef_n = 0, ncoef_i = 0;
+
+  // device inputs
+  DevBuf probe, prop, mask_mid, mask_exit, tw_n, tw_pw, tw_ph, gfsf_d;
+  RowsDev rows_n, rows_i, rows_cn, rows_ci;
+  DevBuf kx_axis, ky_axis, kx, ky, s2, aper_true, cim;
+  // work buffers and results
+  DevBuf T, psi, part, acc, out_result, out_mid;
+  bool t_valid = false;
+  bool has_result = false;
+  int last_what = 0;
+  std::map<PlanKey, cufftHandle> plans;
+
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  TotemTiming timing{};
+  long long h2d_bytes = 0, d2h_bytes = 0;
+  // per-launch profiling of the fused passes (TotemRunOptions.profile)
+  bool profiling = false;
+  std::vector<cudaEvent_t> pev;
+  std::vector<int> pkind;  // 0 = row pass, 1 = column pass
+  size_t pused = 0;
+
+  ~totem_session() {
+    for (auto& kv : plans) cufftDestroy(kv.second);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : pev) cudaEventDestroy(e);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+
+  Status prof_begin() {
+    if (!profiling) return Status::Ok();
+    while (pev.size() < pused + 2) {
+      cudaEvent_t e;
+      TOTEM_CUDA(cudaEventCreate(&e));
+      pev.push_back(e);
+    }
+    TOTEM_CUDA(cudaEventRecord(pev[pused], stream));
+    return Status::Ok();
+  }
+  Status prof_end(int kind) {
+    if (!profiling) return Status::Ok();
+    TOTEM_CUDA(cudaEventRecord(pev[pused + 1], stream));
+    pkind.push_back(kind);
+    pused += 2;
+    return Status::Ok();
+  }
+
+  Status plan(int ph, int pw, int batch, cufftHandle* out) {
+    PlanKey k{ph, pw, batch};
+    auto it = plans.find(k);
+    if (it != plans.end()) {
+      *out = it->second;
+      return Status::Ok();
+    }
+    cufftHandle p;
+    int n[2] = {ph, pw};
+    TOTEM_CUFFT(cufftPlanMany(&p, 2, n, nullptr, 1, ph * pw, nullptr, 1, ph * pw, CUFFT_C2C, batch));
+    TOTEM_CUFFT(cufftSetStream(p, stream));
+    plans[k] = p;
+    *out = p;
+    return Status::Ok();
+  }
+
+  Status upload_args(const TotemStemArgs* a, bool stem);
+  Status build_transmission(int path, int* launches);
+  Status slice_loop(int path, int batch, int* launches, int* batch_used);
+  Status run(int what, const TotemRunOptions* opt);
+  Status collect_timing();
+  Status download(TotemStemOut* out);
+  bool timing_pending = false;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Upload
+// ---------------------------------------------------------------------------------------------
+Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
+  if (a == nullptr) return Status::Err(TOTEM_ERR_INVALID_ARG, "args is NULL");
+  g_h2d_bytes = 0;
+  if (a->struct_size != (int)sizeof(TotemStemArgs))
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "TotemStemArgs.struct_size does not match this library");
+  if (a->param != TOTEM_PARAM_PENG && a->param != TOTEM_PARAM_LOBATO)
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "param must be TOTEM_PARAM_PENG or TOTEM_PARAM_LOBATO");
+  if (a->p_height <= 0 || a->p_width <= 0 || a->slices < 0)
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "negative or zero potential-grid size");
+  if ((a->p_height | a->p_width) & 1)
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "odd grid sizes are not supported (the ifftshift is a quadrant swap)");
+  if (a->layer_len < 0 || a->cim_len < 0) return Status::Err(TOTEM_ERR_INVALID_ARG, "negative count");
+  // The transmission-only MEX receives empty probe / aperture inputs (cuda_stem_potential.m,
+  // HRTEMsimulation sets probe = [] at ToTEM_submit_v1.m:1259); STEM fields are checked only
+  // when a STEM request is present.
+  const bool want_stem = stem && a->depth > 0;
+  stem_ready = false;
+  if (want_stem) {
+    if (a->height <= 0 || a->width <= 0 || a->w_num <= 0 || a->aper_num < 0)
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "negative or zero window size");
+    if ((a->height | a->width) & 1)
+      return Status::Err(TOTEM_ERR_UNSUPPORTED, "odd window sizes are not supported (the ifftshift is a quadrant swap)");
+    if (a->width_red <= 0 || a->step < 0)
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "width_red must be positive and step non-negative");
+    const long last = a->depth - 1;
+    const long rmax = a->begin_row + (last / a->width_red) * (long)a->step;
+    const long cmax = a->begin_col + (long)std::min<long>(last, a->width_red - 1) * a->step;
+    if (a->begin_row < 0 || a->begin_col < 0 || rmax + a->height > a->p_height || cmax + a->width > a->p_width)
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "probe windows leave the potential grid");
+    if (!a->probe_re || !a->probe_im || !a->prop_re || !a->prop_im || !a->gfsf || (a->aper_num > 0 && !a->aper))
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "probe, propagator, gfsf and aper are required for STEM");
+    if (a->layer_len > 0 && (!a->mid_layer || (a->aper_num > 0 && !a->aper2)))
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "mid_layer and aper2 are required when layer_len > 0");
+    if ((long long)a->w_num * a->depth > (1LL << 30)) return Status::Err(TOTEM_ERR_INVALID_ARG, "too many probes");
+  }
+  if (!a->kx || !a->ky || !a->s_2 || !a->aper_true)
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "kx, ky, s_2 and aper_true are required");
+
+  param = a->param;
+  p_h = a->p_height; p_w = a->p_width; slices = a->slices;
+  sigma = a->sigma; parameter = a->parameter;
+  if (want_stem) {
+    h = a->height; w = a->width; depth = a->depth;
+    step = a->step; begin_row = a->begin_row; begin_col = a->begin_col; width_red = a->width_red;
+    w_num = a->w_num; aper_num = a->aper_num;
+    mid_layer.assign(a->mid_layer, a->mid_layer + a->layer_len);
+    gfsf.assign(a->gfsf, a->gfsf + a->w_num);
+  } else {
+    h = w = depth = step = begin_row = begin_col = width_red = aper_num = 0;
+    w_num = 1;
+    mid_layer.clear();
+    gfsf.assign(1, 1.0);
+  }
+  cudaStream_t st = stream;
+  uploaded = false;
+  t_valid = false;
+  has_result = false;
+
+  // coefficient rows
+  const int nc_n = (param == TOTEM_PARAM_LOBATO) ? 14 : 13;
+  const int nc_i = (param == TOTEM_PARAM_LOBATO) ? 26 : 25;
+  std::vector<int> beg_n, beg_i, beg_cn, beg_ci;
+  TOTEM_TRY(offsets(a->atom_slice, slices, beg_n, n_rows, "atom_slice"));
+  TOTEM_TRY(offsets(a->atom_slice_i, slices, beg_i, n_rows_i, "atom_slice_i"));
+  if (n_rows > 0 && !a->proj_coff_mat) return Status::Err(TOTEM_ERR_INVALID_ARG, "proj_coff_mat is NULL");
+  if (n_rows_i > 0 && !a->proj_coff_mat_i) return Status::Err(TOTEM_ERR_INVALID_ARG, "proj_coff_mat_i is NULL");
+  has_abs_n = a->absorp_n != nullptr && n_rows > 0;
+  has_abs_i = a->absorp_n_i != nullptr && n_rows_i > 0;
+  ncoef_n = nc_n - 2;
+  ncoef_i = nc_i - 2;
+  TOTEM_TRY(rows_n.put(split_rows(a->proj_coff_mat, n_rows, nc_n, has_abs_n ? a->absorp_n : nullptr, beg_n), st));
+  TOTEM_TRY(rows_i.put(split_rows(a->proj_coff_mat_i, n_rows_i, nc_i, has_abs_i ? a->absorp_n_i : nullptr, beg_i), st));
+  cim_len = a->cim_len;
+  n_corr = n_corr_i = 0;
+  if (cim_len > 0) {
+    if (!a->corr_info_matrix) return Status::Err(TOTEM_ERR_INVALID_ARG, "corr_info_matrix is NULL");
+    TOTEM_TRY(offsets(a->series_n_corr, slices, beg_cn, n_corr, "series_n_corr"));
+    TOTEM_TRY(offsets(a->series_n_i_corr, slices, beg_ci, n_corr_i, "series_n_i_corr"));
+    if ((n_corr > 0 && !a->ele_n_corr) || (n_corr_i > 0 && !a->ele_n_i_corr))
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "correction rows are NULL");
+    TOTEM_TRY(rows_cn.put(split_rows(a->ele_n_corr, n_corr, 5, nullptr, beg_cn), st));
+    TOTEM_TRY(rows_ci.put(split_rows(a->ele_n_i_corr, n_corr_i, 8, nullptr, beg_ci), st));
+    const size_t plane = (size_t)p_h * p_w;
+    std::vector<float> c(plane * cim_len);
+    for (size_t i = 0; i < c.size(); ++i) c[i] = (float)a->corr_info_matrix[i];
+    TOTEM_TRY(upload(cim, c, st));
+  }
+
+  // reciprocal grids: detect the reference's separable meshgrid layout
+  const size_t plane = (size_t)p_h * p_w;
+  separable = true;
+  for (int r = 0; r < p_h && separable; ++r)
+    for (int c = 0; c < p_w; ++c)
+      if (a->kx[(size_t)r * p_w + c] != a->kx[c] || a->ky[(size_t)r * p_w + c] != a->ky[(size_t)r * p_w]) {
+        separable = false;
+        break;
+      }
+  std::vector<float> s2f(plane);
+  for (size_t i = 0; i < plane; ++i) s2f[i] = (float)a->s_2[i];
+  TOTEM_TRY(upload(s2, s2f, st));
+  if (separable) {
+    std::vector<double> kxa(a->kx, a->kx + p_w), kya(p_h);
+    for (int r = 0; r < p_h; ++r) kya[r] = a->ky[(size_t)r * p_w];
+    TOTEM_TRY(upload(kx_axis, kxa, st));
+    TOTEM_TRY(upload(ky_axis, kya, st));
+  } else {
+    TOTEM_TRY(upload(kx, std::vector<double>(a->kx, a->kx + plane), st));
+    TOTEM_TRY(upload(ky, std::vector<double>(a->ky, a->ky + plane), st));
+  }
+  aper_true_ones = true;
+  for (size_t i = 0; i < plane; ++i)
+    if (a->aper_true[i] != 1.0) {
+      aper_true_ones = false;
+      break;
+    }
+  if (!aper_true_ones) {
+    std::vector<float> at(plane);
+    for (size_t i = 0; i < plane; ++i) at[i] = (float)a->aper_true[i];
+    TOTEM_TRY(upload(aper_true, at, st));
+  }
+  TOTEM_TRY(upload(tw_pw, twiddles(p_w), st));
+  TOTEM_TRY(upload(tw_ph, twiddles(p_h), st));
+
+  // probe, propagator, masks
+  if (want_stem) {
+    const size_t vol = (size_t)h * w;
+    std::vector<float2> pr(vol * w_num), hp(vol);
+    for (size_t i = 0; i < pr.size(); ++i) pr[i] = make_float2((float)a->probe_re[i], (float)a->probe_im[i]);
+    for (size_t i = 0; i < vol; ++i) hp[i] = make_float2((float)a->prop_re[i], (float)a->prop_im[i]);
+    TOTEM_TRY(upload(probe, pr, st));
+    TOTEM_TRY(upload(prop, hp, st));
+    // exit detector: ifftshift(aper) (the reference shifts the wave instead, cuda_source_lobato.cu:1415)
+    std::vector<float> me(vol * std::max(aper_num, 1)), mm;
+    for (int q = 0; q < aper_num; ++q)
+      for (int r = 0; r < h; ++r)
+        for (int c = 0; c < w; ++c)
+          me[(size_t)q * vol + (size_t)r * w + c] =
+              (float)a->aper[(size_t)q * vol + (size_t)((r + h / 2) % h) * w + (c + w / 2) % w];
+    TOTEM_TRY(upload(mask_exit, me, st));
+    if (a->layer_len > 0 && aper_num > 0) {
+      mm.resize(vol * aper_num);
+      for (size_t i = 0; i < mm.size(); ++i) mm[i] = (float)a->aper2[i];
+      TOTEM_TRY(upload(mask_mid, mm, st));
+    }
+    if (h == w) TOTEM_TRY(upload(tw_n, twiddles(h), st));
+    TOTEM_TRY(upload(gfsf_d, gfsf, st));
+  }
+  TOTEM_CUDA(cudaStreamSynchronize(st));  // host staging vectors die at return
+  uploaded = true;
+  stem_ready = want_stem;
+  h2d_bytes = g_h2d_bytes;
+  return Status::Ok();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Transmission
+// ---------------------------------------------------------------------------------------------
+Status totem_session::build_transmission(int path, int* launches) {
+  const size_t plane = (size_t)p_h * p_w;
+  TOTEM_TRY(T.ensure(plane * std::max(slices, 1) * sizeof(float2)));
+  if (slices == 0) return Status::Ok();
+  totem::TxGrid g;
+  g.p_h = p_h; g.p_w = p_w; g.slices = slices;
+  g.separable = separable;
+  g.kx_axis = kx_axis.as<double>(); g.ky_axis = ky_axis.as<double>();
+  g.kx = kx.as<double>(); g.ky = ky.as<double>();
+  g.s2 = s2.as<float>();
+  g.aper_true = aper_true_ones ? nullptr : aper_true.as<float>();
+  g.parameter = (float)parameter;
+  g.lobato = (param == TOTEM_PARAM_LOBATO);
+  g.cim = cim_len > 0 ? cim.as<float>() : nullptr;
+  g.cim_len = cim_len;
+  const auto vn = rows_n.view(n_rows > 0, has_abs_n, ncoef_n);
+  const auto vi = rows_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
+  const auto vcn = rows_cn.view(cim_len > 0 && n_corr > 0, false, 3);
+  const auto vci = rows_ci.view(cim_len > 0 && n_corr_i > 0, false, 6);
+  TOTEM_TRY(totem::launch_tx_structure(g, vn, vi, vcn, vci, T.as<float2>(), stream));
+  ++*launches;
+  const float sig = (float)(sigma / 1000.0);
+  if (path == TOTEM_PATH_FUSED && totem::fused_fft_size_ok(p_h) && totem::fused_fft_size_ok(p_w)) {
+    TOTEM_TRY(totem::launch_tx_fft_exp(T.as<float2>(), slices, p_h, p_w, sig, tw_pw.as<float2>(),
+                                       tw_ph.as<float2>(), stream));
+    *launches += 2;
+  } else {
+    cufftHandle p;
+    TOTEM_TRY(plan(p_h, p_w, slices, &p));
+    TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)T.p, (cufftComplex*)T.p, CUFFT_INVERSE));
+    TOTEM_TRY(totem::launch_sign_exp(T.as<float2>(), (long)plane * slices, p_h, p_w, sig, stream));
+    *launches += 2;
+  }
+  t_valid = true;
+  return Status::Ok();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Slice loop
+// ---------------------------------------------------------------------------------------------
+Status totem_session::slice_loop(int path, int batch, int* launches, int* batch_used) {
+  const long items_total = (long)w_num * depth;
+  const long ad = (long)aper_num * depth;
+  const int L = (int)mid_layer.size();
+  TOTEM_TRY(out_result.ensure(std::max<long>(ad, 1) * sizeof(double)));
+  TOTEM_TRY(out_mid.ensure(std::max<long>(ad * L, 1) * sizeof(double)));
+  if (items_total == 0 || aper_num == 0) {
+    has_result = true;
+    return Status::Ok();
+  }
+  // detection events: every distinct valid mid-layer slice (first occurrence wins, as
+  // find(midslice==k, 1) in cuda_STEM_CPU_Mcore_lobato_peng.m:66-67) plus the exit wave.
+  std::vector<int> event_of_slice(slices + 1, -1);
+  std::vector<int> layer_event(L, -1);
+  int n_events = 0;
+  for (int l = 0; l < L; ++l) {
+    const int k = mid_layer[l];
+    if (k < 1 || k > slices) continue;
+    if (event_of_slice[k] < 0) {
+      event_of_slice[k] = n_events++;
+      layer_event[l] = event_of_slice[k];
+    }
+  }
+  const int exit_event = n_events++;
+
+  const bool fused = (path == TOTEM_PATH_FUSED) && h == w && is_pow2(h) && h >= 64 && h <= 2048 && slices > 0;
+  const size_t vol = (size_t)h * w;
+  int B = batch;
+  if (B <= 0) {
+    const size_t target = fused ? (48u << 20) : (512u << 20);
+    B = (int)std::max<size_t>(1, target / (vol * sizeof(float2)));
+  }
+  B = (int)std::min<long>(B, items_total);
+  {  // spread the items evenly over the batches
+    const long nb = (items_total + B - 1) / B;
+    B = (int)((items_total + nb - 1) / nb);
+  }
+  *batch_used = B;
+  const int nblk = fused ? totem::col_blocks(h) : 64;
+  TOTEM_TRY(psi.ensure((size_t)B * vol * sizeof(float2)));
+  TOTEM_TRY(part.ensure((size_t)n_events * B * aper_num * nblk * sizeof(double)));
+  TOTEM_TRY(acc.ensure((size_t)n_events * w_num * ad * sizeof(double)));
+  TOTEM_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)n_events * w_num * ad * sizeof(double), stream));
+  double* part_e = part.as<double>();
+  const size_t part_stride = (size_t)B * aper_num * nblk;
+  totem::ScanGeom geo{begin_row, begin_col, step, width_red, depth, p_w};
+  const float2* Tp = T.as<float2>();
+  const size_t plane = (size_t)p_h * p_w;
+
+  for (long item0 = 0; item0 < items_total; item0 += B) {
+    const int items = (int)std::min<long>(B, items_total - item0);
+    if (fused) {
+      totem::SliceLoopArgs s;
+      s.n = h; s.items = items; s.item0 = (int)item0; s.geo = geo; s.p_h = p_h;
+      s.psi = psi.as<float2>(); s.probe = probe.as<float2>(); s.prop = prop.as<float2>();
+      s.tw = tw_n.as<float2>(); s.aper_num = aper_num;
+      s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
+      TOTEM_TRY(prof_begin());
+      TOTEM_TRY(totem::launch_row_pass(s, Tp, true, stream));
+      TOTEM_TRY(prof_end(0));
+      ++*launches;
+      for (int k = 0; k < slices; ++k) {
+        const int ev_mid = event_of_slice[k + 1];
+        int flags = 0;
+        if (ev_mid >= 0) {
+          flags |= 1;
+          s.part_mid = part_e + ev_mid * part_stride;
+        }
+        if (k == slices - 1) {
+          flags |= 2 | 4;
+          s.part_exit = part_e + exit_event * part_stride;
+        }
+        TOTEM_TRY(prof_begin());
+        TOTEM_TRY(totem::launch_col_pass(s, flags, stream));
+        TOTEM_TRY(prof_end(1));
+        ++*launches;
+        if (k < slices - 1) {
+          TOTEM_TRY(prof_begin());
+          TOTEM_TRY(totem::launch_row_pass(s, Tp + (size_t)(k + 1) * plane, false, stream));
+          TOTEM_TRY(prof_end(0));
+          ++*launches;
+        }
+      }
+    } else {
+      cufftHandle p;
+      TOTEM_TRY(plan(h, w, items, &p));
+      float2* ps = psi.as<float2>();
+      TOTEM_TRY(totem::launch_plain_init(ps, probe.as<float2>(), h, w, items, (int)item0, depth, stream));
+      ++*launches;
+      for (int k = 0; k < slices; ++k) {
+        TOTEM_TRY(totem::launch_plain_gather_mul(ps, Tp + (size_t)k * plane, h, w, items, (int)item0, geo, stream));
+        TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
+        TOTEM_TRY(totem::launch_plain_mul(ps, prop.as<float2>(), (int)vol, items, stream));
+        *launches += 3;
+        const int ev_mid = event_of_slice[k + 1];
+        if (ev_mid >= 0) {
+          TOTEM_TRY(totem::launch_plain_detect(ps, mask_mid.as<float>(), aper_num, (int)vol, items,
+                                               part_e + ev_mid * part_stride, nblk, stream));
+          ++*launches;
+        }
+        TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_INVERSE));
+        TOTEM_TRY(totem::launch_plain_scale(ps, 1.f / (float)vol, (long)items * vol, stream));
+        *launches += 2;
+      }
+      TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
+      TOTEM_TRY(totem::launch_plain_detect(ps, mask_exit.as<float>(), aper_num, (int)vol, items,
+                                           part_e + exit_event * part_stride, nblk, stream));
+      *launches += 2;
+    }
+    for (int e = 0; e < n_events; ++e) {
+      TOTEM_TRY(totem::launch_det_reduce(part_e + e * part_stride, nblk, aper_num, items, (int)item0, depth,
+                                         acc.as<double>() + (size_t)e * w_num * ad, stream));
+      ++*launches;
+    }
+  }
+  TOTEM_TRY(totem::launch_combine(acc.as<double>() + (size_t)exit_event * w_num * ad, gfsf_d.as<double>(), w_num, ad,
+                                  out_result.as<double>(), stream));
+  ++*launches;
+  if (L > 0) TOTEM_CUDA(cudaMemsetAsync(out_mid.p, 0, (size_t)ad * L * sizeof(double), stream));
+  for (int l = 0; l < L; ++l) {
+    if (layer_event[l] < 0) continue;
+    TOTEM_TRY(totem::launch_combine(acc.as<double>() + (size_t)layer_event[l] * w_num * ad, gfsf_d.as<double>(),
+                                    w_num, ad, out_mid.as<double>() + (size_t)l * ad, stream));
+    ++*launches;
+  }
+  has_result = true;
+  return Status::Ok();
+}
+
+Status totem_session::run(int what, const TotemRunOptions* opt) {
+  if (!uploaded) return Status::Err(TOTEM_ERR_STATE, "run before a successful upload");
+  TotemRunOptions o{};
+  if (opt) o = *opt;
+  if (o.path != TOTEM_PATH_FUSED && o.path != TOTEM_PATH_PLAIN)
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "unknown path");
+  TOTEM_CUDA(cudaSetDevice(device));
+  for (auto& e : ev)
+    if (!e) TOTEM_CUDA(cudaEventCreate(&e));
+  int launches = 0, batch_used = 0;
+  has_result = false;
+  last_what = what;
+  profiling = o.profile != 0;
+  pkind.clear();
+  pused = 0;
+  TOTEM_CUDA(cudaEventRecord(ev[0], stream));
+  if (!(o.skip_transmission && t_valid)) TOTEM_TRY(build_transmission(o.path, &launches));
+  TOTEM_CUDA(cudaEventRecord(ev[1], stream));
+  if (what == 0) {
+    if (!stem_ready && depth > 0) return Status::Err(TOTEM_ERR_STATE, "no STEM inputs uploaded");
+    TOTEM_TRY(slice_loop(o.path, o.batch, &launches, &batch_used));
+  }
+  else has_result = true;
+  TOTEM_CUDA(cudaEventRecord(ev[2], stream));
+  profiling = false;
+  timing = TotemTiming{};
+  timing.kernel_launches = launches;
+  timing.batch = batch_used;
+  timing.probe_slices = (what == 0) ? (long long)w_num * depth * slices : 0;
+  timing.h2d_bytes = h2d_bytes;
+  timing_pending = true;
+  return Status::Ok();
+}
+
+Status totem_session::collect_timing() {
+  if (!timing_pending) return Status::Ok();
+  TOTEM_CUDA(cudaStreamSynchronize(stream));
+  TOTEM_CUDA(cudaEventElapsedTime(&timing.transmission_ms, ev[0], ev[1]));
+  TOTEM_CUDA(cudaEventElapsedTime(&timing.slice_loop_ms, ev[1], ev[2]));
+  TOTEM_CUDA(cudaEventElapsedTime(&timing.total_ms, ev[0], ev[2]));
+  for (size_t i = 0; i < pkind.size(); ++i) {
+    float ms = 0.f;
+    TOTEM_CUDA(cudaEventElapsedTime(&ms, pev[2 * i], pev[2 * i + 1]));
+    if (pkind[i] == 0) {
+      timing.row_pass_ms += ms;
+      ++timing.row_pass_launches;
+    } else {
+      timing.col_pass_ms += ms;
+      ++timing.col_pass_launches;
+    }
+  }
+  timing_pending = false;
+  return Status::Ok();
+}
+
+Status totem_session::download(TotemStemOut* out) {
+  if (!has_result) return Status::Err(TOTEM_ERR_STATE, "no result to download");
+  TOTEM_CUDA(cudaSetDevice(device));
+  TOTEM_TRY(collect_timing());
+  if (out == nullptr) return Status::Ok();
+  const size_t ad = (size_t)aper_num * depth;
+  long long d2h = 0;
+  if (last_what == 0) {
+    if (out->result && ad) {
+      TOTEM_CUDA(cudaMemcpy(out->result, out_result.p, ad * sizeof(double), cudaMemcpyDeviceToHost));
+      d2h += (long long)(ad * sizeof(double));
+    }
+    if (out->mid_layer_mat && ad * mid_layer.size()) {
+      TOTEM_CUDA(cudaMemcpy(out->mid_layer_mat, out_mid.p, ad * mid_layer.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost));
+      d2h += (long long)(ad * mid_layer.size() * sizeof(double));
+    }
+  }
+  if ((out->potential_re || out->potential_im) && t_valid && slices > 0) {
+    const size_t n = (size_t)p_h * p_w * slices;
+    std::vector<float2> t(n);
+    TOTEM_CUDA(cudaMemcpy(t.data(), T.p, n * sizeof(float2), cudaMemcpyDeviceToHost));
+    d2h += (long long)(n * sizeof(float2));
+    for (size_t i = 0; i < n; ++i) {
+      if (out->potential_re) out->potential_re[i] = t[i].x;
+      if (out->potential_im) out->potential_im[i] = t[i].y;
+    }
+  }
+  d2h_bytes = d2h;
+  timing.d2h_bytes = d2h;
+  return Status::Ok();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Device choice and the cached default sessions used by the one-shot entry points
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+Status pick_device(int* dev) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return Status::Err(TOTEM_ERR_NO_DEVICE, "no CUDA device visible");
+  if (*dev >= 0) {
+    if (*dev >= n) return Status::Err(TOTEM_ERR_INVALID_ARG, "device index out of range");
+    return Status::Ok();
+  }
+  size_t best = 0;
+  int bi = 0;
+  for (int i = 0; i < n; ++i) {  // most free memory, as cuda_source_lobato.cu:1071-1081
+    size_t fr = 0, tot = 0;
+    if (cudaSetDevice(i) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr > best) {
+      best = fr;
+      bi = i;
+    }
+  }
+  *dev = bi;
+  return Status::Ok();
+}
+
+Status create_session(int device, void* stream, totem_session** out) {
+  TOTEM_TRY(pick_device(&device));
+  TOTEM_CUDA(cudaSetDevice(device));
+  std::unique_ptr<totem_session> s(new totem_session());
+  s->device = device;
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+  } else {
+    TOTEM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+  }
+  *out = s.release();
+  return Status::Ok();
+}
+
+std::mutex g_default_mu;
+std::map<int, totem_session*> g_default;  // device -> session kept for the one-shot calls
+
+Status default_session(totem_session** out) {
+  int dev = -1;
+  if (const char* e = std::getenv("TOTEM_DEVICE")) dev = std::atoi(e);
+  TOTEM_TRY(pick_device(&dev));
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  auto it = g_default.find(dev);
+  if (it != g_default.end()) {
+    *out = it->second;
+    return Status::Ok();
+  }
+  totem_session* s = nullptr;
+  TOTEM_TRY(create_session(dev, nullptr, &s));
+  g_default[dev] = s;
+  *out = s;
+  return Status::Ok();
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    Status s = f();
+    if (!s.ok()) return fail(s);
+    g_last_error.clear();
+    return TOTEM_OK;
+  } catch (const std::bad_alloc&) {
+    return fail(Status::Err(TOTEM_ERR_OOM, "host allocation failed"));
+  } catch (const std::exception& e) {
+    return fail(Status::Err(TOTEM_ERR_CUDA, e.what()));
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------
+extern "C" {
+
+int totem_abi_version(void) { return TOTEM_ABI_VERSION; }
+
+const char* totem_status_string(int status) {
+  switch (status) {
+    case TOTEM_OK: return "ok";
+    case TOTEM_ERR_INVALID_ARG: return "invalid argument";
+    case TOTEM_ERR_UNSUPPORTED: return "unsupported";
+    case TOTEM_ERR_CUDA: return "CUDA error";
+    case TOTEM_ERR_CUFFT: return "cuFFT error";
+    case TOTEM_ERR_OOM: return "out of memory";
+    case TOTEM_ERR_NO_DEVICE: return "no CUDA device";
+    case TOTEM_ERR_STATE: return "invalid call sequence";
+  }
+  return "unknown status";
+}
+
+const char* totem_last_error(void) { return g_last_error.c_str(); }
+
+int totem_session_create(int device, void* stream, totem_session** out) {
+  if (!out) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "out is NULL"));
+  return guarded([&] { return create_session(device, stream, out); });
+}
+
+int totem_session_destroy(totem_session* s) {
+  if (!s) return TOTEM_OK;
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->stream);
+  delete s;
+  return TOTEM_OK;
+}
+
+int totem_session_upload(totem_session* s, const TotemStemArgs* args) {
+  if (!s) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "session is NULL"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  return guarded([&]() -> Status {
+    TOTEM_CUDA(cudaSetDevice(s->device));
+    return s->upload_args(args, true);
+  });
+}
+
+int totem_session_run(totem_session* s, int what, const TotemRunOptions* opt) {
+  if (!s) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "session is NULL"));
+  if (what != 0 && what != 1) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "what must be 0 or 1"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  return guarded([&] { return s->run(what, opt); });
+}
+
+int totem_session_download(totem_session* s, TotemStemOut* out) {
+  if (!s) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "session is NULL"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  return guarded([&] { return s->download(out); });
+}
+
+int totem_session_timing(totem_session* s, TotemTiming* t) {
+  if (!s || !t) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "NULL argument"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  return guarded([&]() -> Status {
+    TOTEM_CUDA(cudaSetDevice(s->device));
+    TOTEM_TRY(s->collect_timing());
+    *t = s->timing;
+    return Status::Ok();
+  });
+}
+
+int totem_session_transmission(totem_session* s, void** ptr) {
+  if (!s || !ptr) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "NULL argument"));
+  if (!s->t_valid) return fail(Status::Err(TOTEM_ERR_STATE, "no transmission built"));
+  *ptr = s->T.p;
+  return TOTEM_OK;
+}
+
+int totem_stem_run(const TotemStemArgs* args, const TotemRunOptions* opt, TotemStemOut* out) {
+  return guarded([&]() -> Status {
+    totem_session* s = nullptr;
+    TOTEM_TRY(default_session(&s));
+    std::lock_guard<std::mutex> lk(s->mu);
+    TOTEM_CUDA(cudaSetDevice(s->device));
+    TOTEM_TRY(s->upload_args(args, true));
+    TOTEM_TRY(s->run(0, opt));
+    return s->download(out);
+  });
+}
+
+int totem_transmission_run(const TotemStemArgs* args, TotemStemOut* out) {
+  return guarded([&]() -> Status {
+    totem_session* s = nullptr;
+    TOTEM_TRY(default_session(&s));
+    std::lock_guard<std::mutex> lk(s->mu);
+    TOTEM_CUDA(cudaSetDevice(s->device));
+    TOTEM_TRY(s->upload_args(args, false));
+    TOTEM_TRY(s->run(1, nullptr));
+    return s->download(out);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,227 @@
+// Fused multislice: the propagate-and-transmit loop as alternating row and column passes.
+//
+// Reference loop (cuda_source_lobato.cu:1313-1398, CPU form cuda_STEM_CPU_Mcore_lobato_peng.m
+// :60-73), per slice k:  psi *= T_k[window];  Psi = FFT2(psi);  Psi *= H;  [mid detectors];
+// psi = IFFT2(Psi) / N^2.  After the last slice: Psi = FFT2(psi); I_a = sum |Psi|^2 * aper_a.
+//
+// With FFT2 = (row FFT) o (column FFT), consecutive slices regroup into
+//   column pass k : column FFT -> *H -> [detectors] -> column IFFT           (one column at a time)
+//   row pass k+1  : row IFFT -> * T_{k+1}[window] / N^2 -> row FFT           (one row at a time)
+// so every pass reads and writes psi once and keeps a whole row / column in registers and shared
+// memory.  The final FFT2 of the reference cancels the last IFFT2: the exit detectors read the
+// spectrum of the last column pass (after *H), which skips one column IFFT and one row pass.
+//
+// Layout in HBM: psi[item][row][col] complex64, item = w * depth + pos (probe-major, as the
+// reference's w_series loop); T[slice][P_H][P_W]; H[N][N] and the masks [A][N][N] in natural
+// FFT order (the masks for the exit detector are ifftshift(aper), computed at upload).
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace totem {
+
+namespace {
+
+template <int N>
+struct RowCfg {
+  static constexpr int T = N / 8;
+  static constexpr int G = (T >= 256) ? 1 : 256 / T;  // rows per CTA
+};
+template <int N>
+struct ColCfg {
+  static constexpr int T = N / 8;
+  static constexpr int G = (N <= 512) ? 8 : 4;        // columns per CTA
+};
+
+template <int N, int G, bool FIRST>
+__global__ void __launch_bounds__(G * (N / 8)) k_row_pass(SliceLoopArgs a, const float2* __restrict__ tslice, float scale) {
+  extern __shared__ float2 sh[];
+  float2* s_tw = sh;
+  float2* s_x = sh + N;
+  constexpr int T = N / 8;
+  const int g = threadIdx.x / T, j = threadIdx.x - g * T;
+  const long grow = (long)blockIdx.x * G + g;
+  const int item = (int)(grow / N), row = (int)(grow % N);
+  load_twiddles<N>(s_tw, a.tw);
+  const int gi = a.item0 + item;
+  const int w = gi / a.geo.depth, pos = gi - w * a.geo.depth;
+  const int x0 = a.geo.begin_row + (pos / a.geo.width_red) * a.geo.step + row;
+  const int y0 = a.geo.begin_col + (pos % a.geo.width_red) * a.geo.step;
+  const float2* __restrict__ trow = tslice + (long)x0 * a.geo.p_width + y0;
+  float2* prow = a.psi + ((long)item * N + row) * N;
+  float2 v[8];
+  if (FIRST) {
+    const float2* src = a.probe + ((long)w * N + row) * N;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = __ldg(src + j + m * T);
+  } else {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = prow[j + m * T];
+  }
+  __syncthreads();
+  const RowLayout<N> L;
+  if (!FIRST) fft_regs<N, true>(v, j, g, s_tw, s_x, L);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) v[m] = cscale(cmul(v[m], __ldg(trow + j + m * T)), scale);
+  fft_regs<N, false>(v, j, g, s_tw, s_x, L);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) prow[j + m * T] = v[m];
+}
+
+// Deterministic block sum of one double per thread; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double x, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = x;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < nw; ++i) s += red[i];
+  }
+  return s;
+}
+
+template <int N, int G>
+__device__ __forceinline__ void detect(const float (&inten)[8], const float* __restrict__ masks, int aper_num,
+                                       int j, int c, double* __restrict__ part, int item, int cb, int nblk,
+                                       double* red) {
+  constexpr int T = N / 8;
+  for (int a = 0; a < aper_num; ++a) {
+    const float* mk = masks + (long)a * N * N + c;
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc += (double)inten[m] * (double)__ldg(mk + (long)(j + m * T) * N);
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) part[((long)item * aper_num + a) * nblk + cb] = s;
+  }
+}
+
+template <int N, int G>
+__global__ void __launch_bounds__(G * (N / 8)) k_col_pass(SliceLoopArgs a, int flags) {
+  extern __shared__ float2 sh[];
+  float2* s_tw = sh;
+  float2* s_x = sh + N;
+  __shared__ double red[32];
+  constexpr int T = N / 8;
+  constexpr int nblk = N / G;
+  const int j = threadIdx.x / G, g = threadIdx.x - j * G;
+  const int item = blockIdx.x / nblk, cb = blockIdx.x - item * nblk;
+  const int c = cb * G + g;
+  load_twiddles<N>(s_tw, a.tw);
+  float2* base = a.psi + (long)item * N * N + c;
+  float2 v[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) v[m] = base[(long)(j + m * T) * N];
+  __syncthreads();
+  const ColLayout<N, G> L;
+  fft_regs<N, false>(v, j, g, s_tw, s_x, L);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
+  if (flags & 3) {
+    float inten[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) inten[m] = fmaf(v[m].x, v[m].x, v[m].y * v[m].y);
+    if (flags & 1) detect<N, G>(inten, a.mask_mid, a.aper_num, j, c, a.part_mid, item, cb, nblk, red);
+    if (flags & 2) detect<N, G>(inten, a.mask_exit, a.aper_num, j, c, a.part_exit, item, cb, nblk, red);
+  }
+  if (flags & 4) return;
+  fft_regs<N, true>(v, j, g, s_tw, s_x, L);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) base[(long)(j + m * T) * N] = v[m];
+}
+
+__global__ void k_det_reduce(const double* __restrict__ part, int nblk, int aper_num, int items, int item0,
+                             int depth, double* __restrict__ acc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= items * aper_num) return;
+  const int item = t / aper_num, a = t - item * aper_num;
+  const double* p = part + (long)t * nblk;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += p[b];
+  const int gi = item0 + item;
+  const int w = gi / depth, pos = gi - w * depth;
+  acc[((long)w * aper_num + a) * depth + pos] = s;
+}
+
+__global__ void k_combine(const double* __restrict__ acc, const double* __restrict__ gfsf, int w_num, long ad,
+                          double* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= ad) return;
+  double s = 0.0;
+  for (int w = 0; w < w_num; ++w) s += acc[(long)w * ad + i] * gfsf[w];
+  out[i] = s;
+}
+
+template <int N, bool FIRST>
+Status row_pass(const SliceLoopArgs& a, const float2* tslice, cudaStream_t st) {
+  constexpr int G = RowCfg<N>::G, T = RowCfg<N>::T;
+  const size_t smem = sizeof(float2) * (N + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_row_pass<N, G, FIRST>, smem));
+  const long rows = (long)a.items * N;
+  const float scale = FIRST ? 1.f : 1.f / ((float)N * (float)N);
+  k_row_pass<N, G, FIRST><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale);
+  return cuda_status(cudaGetLastError(), "k_row_pass");
+}
+
+template <int N>
+Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
+  constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
+  const size_t smem = sizeof(float2) * (N + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, G>, smem));
+  k_col_pass<N, G><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
+  return cuda_status(cudaGetLastError(), "k_col_pass");
+}
+
+}  // namespace
+
+int col_blocks(int n) {
+  switch (n) {
+    case 64: return 64 / ColCfg<64>::G;
+    case 128: return 128 / ColCfg<128>::G;
+    case 256: return 256 / ColCfg<256>::G;
+    case 512: return 512 / ColCfg<512>::G;
+    case 1024: return 1024 / ColCfg<1024>::G;
+    case 2048: return 2048 / ColCfg<2048>::G;
+  }
+  return 0;
+}
+
+Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st) {
+  switch (a.n) {
+#define TOTEM_ROW(NN) \
+  case NN: return first ? row_pass<NN, true>(a, tslice, st) : row_pass<NN, false>(a, tslice, st);
+    TOTEM_ROW(64) TOTEM_ROW(128) TOTEM_ROW(256) TOTEM_ROW(512) TOTEM_ROW(1024) TOTEM_ROW(2048)
+#undef TOTEM_ROW
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused slice loop needs a power-of-two window 64..2048");
+}
+
+Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
+  switch (a.n) {
+    case 64: return col_pass<64>(a, flags, st);
+    case 128: return col_pass<128>(a, flags, st);
+    case 256: return col_pass<256>(a, flags, st);
+    case 512: return col_pass<512>(a, flags, st);
+    case 1024: return col_pass<1024>(a, flags, st);
+    case 2048: return col_pass<2048>(a, flags, st);
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused slice loop needs a power-of-two window 64..2048");
+}
+
+Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth, double* acc,
+                         cudaStream_t st) {
+  const int n = items * aper_num;
+  if (n == 0) return Status::Ok();
+  k_det_reduce<<<(n + 127) / 128, 128, 0, st>>>(part, nblk, aper_num, items, item0, depth, acc);
+  return cuda_status(cudaGetLastError(), "k_det_reduce");
+}
+
+Status launch_combine(const double* acc, const double* gfsf, int w_num, long ad, double* out, cudaStream_t st) {
+  if (ad == 0) return Status::Ok();
+  k_combine<<<(unsigned)((ad + 255) / 256), 256, 0, st>>>(acc, gfsf, w_num, ad, out);
+  return cuda_status(cudaGetLastError(), "k_combine");
+}
+
+}  // namespace totem

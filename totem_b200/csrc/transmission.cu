@@ -1,0 +1,307 @@
+// Transmission builder: per-slice projected potential in Fourier space, inverse 2-D FFT, and
+// T = exp(i * sigma/1000 * V).
+//
+// Reference: cal_p / initKernel_P (cuda_source_lobato.cu:585-956, cuda_source_peng_and_corr.cu
+// :785-1156) and the correction potential p_corr (cuda_source_peng_and_corr.cu:587-779); the CPU
+// statement of the same sums is GetPotential4AllSlice_multicore_lotabo_peng(_corr).m.
+//
+// Differences by design:
+//  * one thread owns each pixel's accumulator for all atoms of a slice (the reference launches
+//    one thread per (atom, pixel) and adds into the same pixel without atomics,
+//    cuda_source_lobato.cu:82-83);
+//  * the phase exp(-2 pi i (kx x + ky y)) is reduced modulo one in FP64 before the FP32
+//    sincospi (the reference forms the angle in FP32 with pi = 3.14159265, :80-81); on the
+//    reference's separable grids the two factors are tabulated per atom and tile;
+//  * the ifftshift before the inverse FFT is folded into a (-1)^(r+c) factor after it, and
+//    APERTURE is applied while the sum is written.
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace totem {
+
+namespace {
+
+constexpr int TX_TC = 32;      // tile columns (one per lane)
+constexpr int TX_PR = 4;       // rows per thread
+constexpr int TX_TR = 32;      // tile rows (8 warps x 4)
+constexpr int TX_CH = 32;      // atoms staged per chunk
+constexpr int TX_MAXC = 24;    // widest coefficient block (ionic Lobato row without x, y)
+
+__device__ __forceinline__ float peng5(const float* c, float s2) {
+  float f = 0.f;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) f = fmaf(c[2 * i], __expf(-c[2 * i + 1] * s2), f);
+  return f;
+}
+
+__device__ __forceinline__ float lobato5(const float* c, float g2) {
+  float f = 0.f;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const float b = c[2 * i + 1];
+    const float d = fmaf(b, g2, 1.f);
+    f = fmaf(c[2 * i], __fdividef(fmaf(b, g2, 2.f), d * d), f);
+  }
+  return f;
+}
+
+// exp(-2 pi i t) for t given in FP64, reduced to [0, 1) before the FP32 evaluation.
+__device__ __forceinline__ float2 phase_of(double t) {
+  const double fr = t - floor(t);
+  float s, c;
+  sincospif(2.f * (float)fr, &s, &c);
+  return make_float2(c, -s);
+}
+
+struct TxSmem {
+  double pos[TX_CH][2];
+  float coef[TX_CH][TX_MAXC];
+  float absorp[TX_CH][10];
+  float2 ex[TX_CH][TX_TC];
+  float2 ey[TX_CH][TX_TR];
+};
+
+// kind: 0 neutral, 1 ionic, 2 correction (neutral), 3 correction (ionic)
+template <bool SEP>
+__device__ void accumulate_rows(const TxGrid& g, const AtomRowsDev& rows, int kind, int slice, TxSmem& sm,
+                                int tx, int ty, int c, int r0, int c_tile, int r_tile, const float* s2v,
+                                const double* kxv, const double* kyv, const int* pix, float2* acc) {
+  if (rows.beg == nullptr) return;
+  const int a_begin = rows.beg[slice], a_end = rows.beg[slice + 1];
+  const long plane = (long)g.p_h * g.p_w;
+  for (int a0 = a_begin; a0 < a_end; a0 += TX_CH) {
+    const int na = min(TX_CH, a_end - a0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < na * 2; e += blockDim.x) sm.pos[e >> 1][e & 1] = rows.pos[(long)(a0 + (e >> 1)) * 2 + (e & 1)];
+    for (int e = threadIdx.x; e < na * rows.ncoef; e += blockDim.x) {
+      const int a = e / rows.ncoef, k = e - a * rows.ncoef;
+      sm.coef[a][k] = rows.coef[(long)(a0 + a) * rows.ncoef + k];
+    }
+    if (rows.absorp != nullptr)
+      for (int e = threadIdx.x; e < na * 10; e += blockDim.x) sm.absorp[e / 10][e % 10] = rows.absorp[(long)a0 * 10 + e];
+    __syncthreads();
+    if (SEP) {
+      for (int e = threadIdx.x; e < na * (TX_TC + TX_TR); e += blockDim.x) {
+        const int a = e / (TX_TC + TX_TR), k = e - a * (TX_TC + TX_TR);
+        if (k < TX_TC) {
+          const int cc = min(c_tile + k, g.p_w - 1);
+          sm.ex[a][k] = phase_of(g.kx_axis[cc] * sm.pos[a][0]);
+        } else {
+          const int rr = min(r_tile + k - TX_TC, g.p_h - 1);
+          sm.ey[a][k - TX_TC] = phase_of(g.ky_axis[rr] * sm.pos[a][1]);
+        }
+      }
+      __syncthreads();
+    }
+    for (int a = 0; a < na; ++a) {
+      const float* cf = sm.coef[a];
+      float2 ex = make_float2(1.f, 0.f);
+      if (SEP) ex = sm.ex[a][tx];
+#pragma unroll
+      for (int i = 0; i < TX_PR; ++i) {
+        const float s2 = s2v[i];
+        float2 ph;
+        if (SEP) ph = cmul(ex, sm.ey[a][ty * TX_PR + i]);
+        else ph = phase_of(kxv[i] * sm.pos[a][0] + kyv[i] * sm.pos[a][1]);
+        float fr, fi = 0.f;
+        if (kind == 0) {
+          if (g.lobato) fr = cf[0] * lobato5(cf + 1, 4.f * s2) * __expf(-cf[11] * s2);
+          else fr = cf[0] * peng5(cf + 1, s2);
+          if (rows.absorp != nullptr) fi = cf[0] * peng5(sm.absorp[a], s2);
+        } else if (kind == 1) {
+          if (g.lobato)
+            fr = cf[0] * (cf[1] * lobato5(cf + 2, 4.f * s2) + cf[12] * lobato5(cf + 13, 4.f * s2)) *
+                 __expf(-cf[23] * s2);
+          else fr = cf[0] * (cf[1] * peng5(cf + 2, s2) + cf[12] * peng5(cf + 13, s2));
+          if (rows.absorp != nullptr) fi = cf[0] * peng5(sm.absorp[a], s2);
+        } else if (kind == 2) {
+          const int idx = (int)cf[2] - 1;
+          const float m = (idx >= 0 && idx < g.cim_len && pix[i] >= 0) ? g.cim[idx * plane + pix[i]] : 0.f;
+          fr = cf[1] * m * __expf(-cf[0] * s2);
+        } else {
+          const int i1 = (int)cf[3] - 1, i2 = (int)cf[5] - 1;
+          float m = 0.f;
+          if (pix[i] >= 0) {
+            if (i1 >= 0 && i1 < g.cim_len) m = fmaf(cf[2], g.cim[i1 * plane + pix[i]], m);
+            if (i2 >= 0 && i2 < g.cim_len) m = fmaf(cf[4], g.cim[i2 * plane + pix[i]], m);
+          }
+          fr = cf[1] * m * __expf(-cf[0] * s2);
+        }
+        acc[i].x = fmaf(fr, ph.x, fmaf(-fi, ph.y, acc[i].x));
+        acc[i].y = fmaf(fr, ph.y, fmaf(fi, ph.x, acc[i].y));
+      }
+    }
+  }
+}
+
+template <bool SEP>
+__global__ void __launch_bounds__(256) k_tx_structure(TxGrid g, AtomRowsDev nr, AtomRowsDev ir, AtomRowsDev cn,
+                                                      AtomRowsDev ci, float2* __restrict__ out) {
+  __shared__ TxSmem sm;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int slice = blockIdx.z;
+  const int c_tile = blockIdx.x * TX_TC, r_tile = blockIdx.y * TX_TR;
+  const int c = c_tile + tx, r0 = r_tile + ty * TX_PR;
+  float s2v[TX_PR];
+  double kxv[TX_PR], kyv[TX_PR];
+  int pix[TX_PR];
+  float2 acc[TX_PR];
+#pragma unroll
+  for (int i = 0; i < TX_PR; ++i) {
+    const int r = r0 + i;
+    const bool in = (r < g.p_h) && (c < g.p_w);
+    pix[i] = in ? r * g.p_w + c : -1;
+    s2v[i] = in ? g.s2[pix[i]] : 0.f;
+    kxv[i] = (!SEP && in) ? g.kx[pix[i]] : 0.0;
+    kyv[i] = (!SEP && in) ? g.ky[pix[i]] : 0.0;
+    acc[i] = make_float2(0.f, 0.f);
+  }
+  accumulate_rows<SEP>(g, nr, 0, slice, sm, tx, ty, c, r0, c_tile, r_tile, s2v, kxv, kyv, pix, acc);
+  accumulate_rows<SEP>(g, ir, 1, slice, sm, tx, ty, c, r0, c_tile, r_tile, s2v, kxv, kyv, pix, acc);
+  accumulate_rows<SEP>(g, cn, 2, slice, sm, tx, ty, c, r0, c_tile, r_tile, s2v, kxv, kyv, pix, acc);
+  accumulate_rows<SEP>(g, ci, 3, slice, sm, tx, ty, c, r0, c_tile, r_tile, s2v, kxv, kyv, pix, acc);
+  float2* dst = out + (long)slice * g.p_h * g.p_w;
+#pragma unroll
+  for (int i = 0; i < TX_PR; ++i) {
+    if (pix[i] < 0) continue;
+    const float ap = (g.aper_true != nullptr) ? g.aper_true[pix[i]] : 1.f;
+    dst[pix[i]] = cscale(acc[i], g.parameter * ap);
+  }
+}
+
+// In-place inverse FFT of rows of length N (N/8 threads per row, G rows per CTA).
+template <int N, int G>
+__global__ void __launch_bounds__(G * (N / 8)) k_fft_rows_inv(float2* __restrict__ data, const float2* __restrict__ tw) {
+  extern __shared__ float2 sh[];
+  float2* s_tw = sh;
+  float2* s_x = sh + N;
+  constexpr int T = N / 8;
+  const int g = threadIdx.x / T, j = threadIdx.x - g * T;
+  const long row = (long)blockIdx.x * G + g;
+  load_twiddles<N>(s_tw, tw);
+  float2* p = data + row * N;
+  float2 v[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) v[m] = p[j + m * T];
+  __syncthreads();
+  fft_regs<N, true>(v, j, g, s_tw, s_x, RowLayout<N>());
+#pragma unroll
+  for (int m = 0; m < 8; ++m) p[j + m * T] = v[m];
+}
+
+// Column inverse FFT of length N over a p_w-wide plane, (-1)^(r+c), exp(i s V).
+template <int N, int G>
+__global__ void __launch_bounds__(G * (N / 8)) k_fft_cols_exp(float2* __restrict__ data, int p_w,
+                                                             const float2* __restrict__ tw, float sig) {
+  extern __shared__ float2 sh[];
+  float2* s_tw = sh;
+  float2* s_x = sh + N;
+  constexpr int T = N / 8;
+  const int j = threadIdx.x / G, g = threadIdx.x - j * G;
+  const int nblk = p_w / G;
+  const int slice = blockIdx.x / nblk, cb = blockIdx.x - slice * nblk;
+  const int c = cb * G + g;
+  load_twiddles<N>(s_tw, tw);
+  float2* p = data + (long)slice * N * p_w + c;
+  float2 v[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) v[m] = p[(long)(j + m * T) * p_w];
+  __syncthreads();
+  fft_regs<N, true>(v, j, g, s_tw, s_x, ColLayout<N, G>());
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int r = j + m * T;
+    const float sgn = ((r + c) & 1) ? -1.f : 1.f;
+    const float re = sgn * v[m].x * sig, im = sgn * v[m].y * sig;
+    const float amp = expf(-im);
+    float sn, cs;
+    sincosf(re, &sn, &cs);
+    p[(long)r * p_w] = make_float2(amp * cs, amp * sn);
+  }
+}
+
+__global__ void k_sign_exp(float2* __restrict__ data, long total, int p_h, int p_w, float sig) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long plane = (long)p_h * p_w;
+    const long k = i % plane;
+    const int r = (int)(k / p_w), c = (int)(k % p_w);
+    // ifftshift of the input == multiplication of the output by (-1)^(r+c) (even sizes only;
+    // the uploader rejects odd grids, as the reference's quadrant-swap ifftShift assumes).
+    const float sgn = ((r + c) & 1) ? -1.f : 1.f;
+    float2 v = data[i];
+    const float re = sgn * v.x * sig, im = sgn * v.y * sig;
+    const float amp = expf(-im);
+    float sn, cs;
+    sincosf(re, &sn, &cs);
+    data[i] = make_float2(amp * cs, amp * sn);
+  }
+}
+
+template <int N>
+Status rows_inv(float2* data, long nrows, const float2* tw, cudaStream_t st) {
+  constexpr int T = N / 8;
+  constexpr int G = (T >= 256) ? 1 : 256 / T;
+  const size_t smem = sizeof(float2) * (N + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_fft_rows_inv<N, G>, smem));
+  k_fft_rows_inv<N, G><<<(unsigned)(nrows / G), G * T, smem, st>>>(data, tw);
+  return cuda_status(cudaGetLastError(), "k_fft_rows_inv");
+}
+
+template <int N>
+Status cols_exp(float2* data, int slices, int p_w, const float2* tw, float sig, cudaStream_t st) {
+  constexpr int T = N / 8;
+  constexpr int G = (N <= 512) ? 8 : (N <= 2048 ? 4 : 2);
+  const size_t smem = sizeof(float2) * (N + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_fft_cols_exp<N, G>, smem));
+  if (p_w % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "potential width not a multiple of the column tile");
+  k_fft_cols_exp<N, G><<<(unsigned)((long)slices * (p_w / G)), G * T, smem, st>>>(data, p_w, tw, sig);
+  return cuda_status(cudaGetLastError(), "k_fft_cols_exp");
+}
+
+}  // namespace
+
+bool fused_fft_size_ok(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; }
+
+Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const AtomRowsDev& ion,
+                           const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out, cudaStream_t st) {
+  dim3 grid((g.p_w + TX_TC - 1) / TX_TC, (g.p_h + TX_TR - 1) / TX_TR, g.slices);
+  if (g.slices == 0) return Status::Ok();
+  if (g.separable) k_tx_structure<true><<<grid, 256, 0, st>>>(g, neutral, ion, corr_n, corr_i, out);
+  else k_tx_structure<false><<<grid, 256, 0, st>>>(g, neutral, ion, corr_n, corr_i, out);
+  return cuda_status(cudaGetLastError(), "k_tx_structure");
+}
+
+Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sig, const float2* tw_w,
+                         const float2* tw_h, cudaStream_t st) {
+  if (!fused_fft_size_ok(p_h) || !fused_fft_size_ok(p_w))
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused transmission builder needs power-of-two grids 64..4096");
+  const long nrows = (long)slices * p_h;
+  switch (p_w) {
+    case 64: TOTEM_TRY(rows_inv<64>(data, nrows, tw_w, st)); break;
+    case 128: TOTEM_TRY(rows_inv<128>(data, nrows, tw_w, st)); break;
+    case 256: TOTEM_TRY(rows_inv<256>(data, nrows, tw_w, st)); break;
+    case 512: TOTEM_TRY(rows_inv<512>(data, nrows, tw_w, st)); break;
+    case 1024: TOTEM_TRY(rows_inv<1024>(data, nrows, tw_w, st)); break;
+    case 2048: TOTEM_TRY(rows_inv<2048>(data, nrows, tw_w, st)); break;
+    case 4096: TOTEM_TRY(rows_inv<4096>(data, nrows, tw_w, st)); break;
+  }
+  switch (p_h) {
+    case 64: return cols_exp<64>(data, slices, p_w, tw_h, sig, st);
+    case 128: return cols_exp<128>(data, slices, p_w, tw_h, sig, st);
+    case 256: return cols_exp<256>(data, slices, p_w, tw_h, sig, st);
+    case 512: return cols_exp<512>(data, slices, p_w, tw_h, sig, st);
+    case 1024: return cols_exp<1024>(data, slices, p_w, tw_h, sig, st);
+    case 2048: return cols_exp<2048>(data, slices, p_w, tw_h, sig, st);
+    case 4096: return cols_exp<4096>(data, slices, p_w, tw_h, sig, st);
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "grid size");
+}
+
+Status launch_sign_exp(float2* data, long total, int p_h, int p_w, float sig, cudaStream_t st) {
+  if (total == 0) return Status::Ok();
+  int blocks = (int)std::min<long>((total + 255) / 256, 148L * 16);
+  k_sign_exp<<<blocks, 256, 0, st>>>(data, total, p_h, p_w, sig);
+  return cuda_status(cudaGetLastError(), "k_sign_exp");
+}
+
+}  // namespace totem

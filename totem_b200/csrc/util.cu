@@ -1,0 +1,88 @@
+// Status helpers and the small conversion kernels used while uploading a request.
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "common.cuh"
+
+namespace totem {
+
+Status cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return Status::Ok();
+  const int code = (e == cudaErrorMemoryAllocation) ? TOTEM_ERR_OOM
+                   : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? TOTEM_ERR_NO_DEVICE
+                                                                                   : TOTEM_ERR_CUDA;
+  return Status::Err(code, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+Status cufft_status(cufftResult r, const char* what) {
+  if (r == CUFFT_SUCCESS) return Status::Ok();
+  const int code = (r == CUFFT_ALLOC_FAILED) ? TOTEM_ERR_OOM : TOTEM_ERR_CUFFT;
+  return Status::Err(code, std::string(what) + ": cufftResult " + std::to_string((int)r));
+}
+
+Status ensure_smem(const void* func, size_t bytes) {
+  if (bytes <= 48 * 1024) return Status::Ok();
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;  // one entry per (kernel, device)
+  int dev = 0;
+  TOTEM_CUDA(cudaGetDevice(&dev));
+  const auto key = std::make_pair(func, dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return Status::Ok();
+  TOTEM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done[key] = bytes;
+  return Status::Ok();
+}
+
+namespace {
+
+__global__ void k_d2f2(const double* __restrict__ re, const double* __restrict__ im, float2* __restrict__ out,
+                       long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = make_float2((float)re[i], im ? (float)im[i] : 0.f);
+}
+
+__global__ void k_d2f(const double* __restrict__ in, float* __restrict__ out, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+// out[a][r][c] = aper[a][(r + shift) % h][(c + shift') % w]; shift = 1 gives ifftshift for even
+// sizes (the quadrant swap the reference applies to the exit wave, cuda_source_lobato.cu:210-253).
+__global__ void k_shift_masks(const double* __restrict__ aper, float* __restrict__ out, int aper_num, int h, int w,
+                              int shift) {
+  const long total = (long)aper_num * h * w;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int a = (int)(i / ((long)h * w));
+    const int e = (int)(i % ((long)h * w)), r = e / w, c = e % w;
+    const int rs = shift ? (r + h / 2) % h : r, cs = shift ? (c + w / 2) % w : c;
+    out[i] = (float)aper[(long)a * h * w + (long)rs * w + cs];
+  }
+}
+
+inline int grid_for(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 16); }
+
+}  // namespace
+
+Status launch_d2f2(const double* re, const double* im, float2* out, long n, cudaStream_t st) {
+  if (n == 0) return Status::Ok();
+  k_d2f2<<<grid_for(n), 256, 0, st>>>(re, im, out, n);
+  return cuda_status(cudaGetLastError(), "k_d2f2");
+}
+
+Status launch_d2f(const double* in, float* out, long n, cudaStream_t st) {
+  if (n == 0) return Status::Ok();
+  k_d2f<<<grid_for(n), 256, 0, st>>>(in, out, n);
+  return cuda_status(cudaGetLastError(), "k_d2f");
+}
+
+Status launch_shift_masks(const double* aper, float* out, int aper_num, int h, int w, int shift, cudaStream_t st) {
+  const long n = (long)aper_num * h * w;
+  if (n == 0) return Status::Ok();
+  k_shift_masks<<<grid_for(n), 256, 0, st>>>(aper, out, aper_num, h, w, shift);
+  return cuda_status(cudaGetLastError(), "k_shift_masks");
+}
+
+}  // namespace totem
