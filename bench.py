@@ -239,7 +239,9 @@ def main():
     from totem_b200 import capi
     path = capi.PATH_FUSED if ns.path == "fused" else capi.PATH_PLAIN
     req = build_workload(ns.workload)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the engine launches on it and the CUDA events below are recorded on it
+    # (the legacy default stream has handle 0, which the C ABI reads as "make your own stream")
+    stream = torch.cuda.Stream()
     sess = capi.Session(device=local, stream=stream.cuda_stream)
     sess.upload(req)
 

@@ -47,6 +47,15 @@ def test_stem_window_sizes(engine_lib, n, p):
     _check(req, res, mid)
 
 
+@pytest.mark.parametrize("n,p,raster,step", [(512, 1024, (2, 2), 64), (1024, 1024, (1, 1), 0)])
+def test_stem_large_windows(engine_lib, n, p, raster, step):
+    req = request.build_small_stem(n=n, p=p, raster=raster, step=step, slices=3, sampling=0.05, cells=4,
+                                   mid_layer=(2,))
+    for path in (capi.PATH_FUSED, capi.PATH_PLAIN):
+        res, mid = capi.stem_run(req, path=path)
+        _check(req, res, mid)
+
+
 def test_transmission_vs_oracle(engine_lib):
     req = request.build_small_stem(flag="l")
     t = capi.transmission_run(req)

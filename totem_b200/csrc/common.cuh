@@ -4,6 +4,7 @@
 #include <cufft.h>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/totem_b200.h"
 
@@ -89,6 +90,8 @@ Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sigma
 Status launch_sign_exp(float2* data, long total, int p_h, int p_w, float sigma_scaled, cudaStream_t st);
 
 bool fused_fft_size_ok(int n);
+// Per-stage twiddle tables of the shared-memory FFT of length n (empty if n is unsupported).
+std::vector<float2> stage_twiddles(int n);
 
 // ---------------------------------------------------------------------------------------------
 // Fused multislice

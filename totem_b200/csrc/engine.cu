@@ -64,12 +64,11 @@ Status upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
   return Status::Ok();
 }
 
+// Stage twiddle tables of the shared-memory FFT (a one-entry placeholder for sizes it does not
+// handle; those sizes go through cuFFT).
 std::vector<float2> twiddles(int n) {
-  std::vector<float2> t(n);
-  for (int e = 0; e < n; ++e) {
-    const double a = -2.0 * M_PI * (double)e / (double)n;
-    t[e] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
+  std::vector<float2> t = totem::stage_twiddles(n);
+  if (t.empty()) t.assign(1, make_float2(1.f, 0.f));
   return t;
 }
 

@@ -1,209 +1,398 @@
 // Shared-memory Stockham FFT building blocks for sm_100a.
 //
-// A length-N transform (N = 8^k * {1,2,4}, 64 <= N <= 4096) is executed by T = N/8 threads.
-// Each thread holds 8 points in registers.  On entry and on exit thread j holds the elements
-// at positions j + m*T (m = 0..7), so an inverse transform followed by a point-wise multiply and
-// a forward transform never leaves registers between the two transforms.  Stages exchange data
-// through a caller-provided shared-memory region; the caller chooses the region's address map
-// (row-major with padding for contiguous rows, column-interleaved for strided columns).
+// A length-N transform is executed by T = N/P threads that each hold P points in registers.
+// On entry and on exit thread j holds the elements at positions j + m*T (m = 0..P-1), so an
+// inverse transform followed by a point-wise multiply and a forward transform never leaves
+// registers between the two transforms.
 //
-// Radix sequence: radix-8 stages first, then one radix-2 or radix-4 stage when N is not a power
-// of 8.  Twiddles W_N^e = exp(-2 pi i e / N) come from a table computed on the host in FP64 and
-// rounded once to FP32 (table index e in [0, N)); the inverse uses their conjugates.
+// Plans (radices per stage, first stage first):
+//   N   :  64    128     256      512      1024     2048       4096
+//   P   :  8     16      16       32       32       32         32
+//   R   :  8x8   16x8    16x16    32x16    32x32    32x8x8     32x16x8
+// so N <= 1024 needs one shared-memory exchange per transform.  Radix-16 and radix-32
+// butterflies run in registers as 4x4 and 8x4 Cooley-Tukey splits whose internal twiddles are
+// compile-time constants.  Inter-stage twiddles W_N^e = exp(-2 pi i e / N) come from per-stage
+// tables (index (r-1)*Ns + k) computed on the host in FP64, rounded once to FP32 and staged in
+// shared memory; lanes with consecutive k read consecutive entries, so the reads are free of bank
+// conflicts.  Exchanges use XOR-swizzled addresses chosen so that every 64-bit store and load of
+// a half-warp hits distinct banks.
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace totem {
 
+// Complex arithmetic on (re, im) pairs with sm_100's packed FP32 instructions (two IEEE FP32
+// operations per lane, round-to-nearest, the same results as the scalar forms).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+// a * b = a.x * (b.x, b.y) + a.y * (-b.y, b.x)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+  return __ffma2_rn(make_float2(a.x, a.x), b, __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x)));
 }
-// a * conj(b)
+// a * conj(b) = a.x * (b.x, -b.y) + a.y * (b.y, b.x)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+  return __ffma2_rn(make_float2(a.x, a.x), make_float2(b.x, -b.y), __fmul2_rn(make_float2(a.y, a.y), make_float2(b.y, b.x)));
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-// multiply by -i (forward) or +i (inverse)
-template <bool INV>
-__device__ __forceinline__ float2 mul_mi(float2 a) {
-  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+// a + s * (-i b) for s = +1 / -1 (forward) or a + s * (+i b) (inverse): the radix-4 cross term
+template <bool INV, int S>
+__device__ __forceinline__ float2 cadd_rot(float2 a, float2 b) {
+  // -i b = (b.y, -b.x), +i b = (-b.y, b.x)
+  constexpr float sx = (INV ? -1.f : 1.f) * S, sy = (INV ? 1.f : -1.f) * S;
+  return __ffma2_rn(make_float2(b.y, b.x), make_float2(sx, sy), a);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Small DFTs on registers, natural order in and out.
+// Compile-time trigonometry for the butterflies' internal twiddles (Taylor series in double,
+// argument reduced to |x| <= pi/4; exact multiples of 2 pi / R only).
+// ---------------------------------------------------------------------------------------------
+constexpr double kPi = 3.14159265358979323846;
+constexpr double ce_poly_sin(double x) {
+  double t = x, s = x;
+  for (int k = 1; k < 12; ++k) {
+    t = -t * x * x / ((2 * k) * (2 * k + 1));
+    s += t;
+  }
+  return s;
+}
+constexpr double ce_poly_cos(double x) {
+  double t = 1.0, s = 1.0;
+  for (int k = 1; k < 12; ++k) {
+    t = -t * x * x / ((2 * k - 1) * (2 * k));
+    s += t;
+  }
+  return s;
+}
+// cos / sin of 2 pi e / R via octant symmetry
+constexpr double ce_cos_frac(int e, int R) {
+  e = ((e % R) + R) % R;
+  const int o8 = (8 * e) / R;  // octant index 0..7
+  const double x = 2 * kPi * e / R;
+  switch (o8) {
+    case 0: return ce_poly_cos(x);
+    case 1: return ce_poly_sin(kPi / 2 - x);
+    case 2: return -ce_poly_sin(x - kPi / 2);
+    case 3: return -ce_poly_cos(kPi - x);
+    case 4: return -ce_poly_cos(x - kPi);
+    case 5: return -ce_poly_sin(3 * kPi / 2 - x);
+    case 6: return ce_poly_sin(x - 3 * kPi / 2);
+    default: return ce_poly_cos(2 * kPi - x);
+  }
+}
+constexpr double ce_sin_frac(int e, int R) { return ce_cos_frac(e - R / 4, R); }
+
+// x * W_R^e (forward: exp(-2 pi i e/R)); inverse uses the conjugate.  Trivial angles are exact.
+template <int E, int R, bool INV>
+__device__ __forceinline__ float2 twiddle_const(float2 x) {
+  constexpr int e = ((E % R) + R) % R;
+  constexpr float r2 = 0.70710678118654752440f;
+  if constexpr (e == 0) {
+    return x;
+  } else if constexpr (4 * e == R) {  // -i (forward)
+    return INV ? make_float2(-x.y, x.x) : make_float2(x.y, -x.x);
+  } else if constexpr (2 * e == R) {
+    return make_float2(-x.x, -x.y);
+  } else if constexpr (4 * e == 3 * R) {  // +i (forward)
+    return INV ? make_float2(x.y, -x.x) : make_float2(-x.y, x.x);
+  } else if constexpr (8 * e == R) {  // (1 -/+ i)/sqrt2 = (x + rot x) / sqrt2
+    return cscale(cadd_rot<INV, 1>(x, x), r2);
+  } else if constexpr (8 * e == 3 * R) {  // (-1 -/+ i)/sqrt2
+    return cscale(cadd_rot<INV, 1>(make_float2(-x.x, -x.y), x), r2);
+  } else if constexpr (8 * e == 5 * R) {  // (-1 +/- i)/sqrt2
+    return cscale(cadd_rot<INV, -1>(make_float2(-x.x, -x.y), x), r2);
+  } else if constexpr (8 * e == 7 * R) {  // (1 +/- i)/sqrt2
+    return cscale(cadd_rot<INV, -1>(x, x), r2);
+  } else {
+    constexpr float c = (float)ce_cos_frac(e, R);
+    constexpr float s = INV ? (float)ce_sin_frac(e, R) : -(float)ce_sin_frac(e, R);
+    return cmul(x, make_float2(c, s));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Register DFTs, natural order in and out.
 // ---------------------------------------------------------------------------------------------
 template <bool INV>
-__device__ __forceinline__ void dft2(float2& a, float2& b) {
-  float2 t = a;
-  a = cadd(t, b);
-  b = csub(t, b);
+__device__ __forceinline__ void dft2(float2* x) {
+  const float2 t = x[0];
+  x[0] = cadd(t, x[1]);
+  x[1] = csub(t, x[1]);
 }
 
 template <bool INV>
-__device__ __forceinline__ void dft4(float2& y0, float2& y1, float2& y2, float2& y3) {
-  float2 b0 = cadd(y0, y2), b1 = csub(y0, y2);
-  float2 b2 = cadd(y1, y3), b3 = mul_mi<INV>(csub(y1, y3));
-  y0 = cadd(b0, b2);
-  y2 = csub(b0, b2);
-  y1 = cadd(b1, b3);
-  y3 = csub(b1, b3);
+__device__ __forceinline__ void dft4(float2* y) {
+  const float2 b0 = cadd(y[0], y[2]), b1 = csub(y[0], y[2]);
+  const float2 b2 = cadd(y[1], y[3]);
+  const float2 d = csub(y[1], y[3]);
+  y[0] = cadd(b0, b2);
+  y[2] = csub(b0, b2);
+  y[1] = cadd_rot<INV, 1>(b1, d);   // b1 + (-/+ i) d
+  y[3] = cadd_rot<INV, -1>(b1, d);  // b1 - (-/+ i) d
 }
 
 template <bool INV>
 __device__ __forceinline__ void dft8(float2* x) {
-  const float r = 0.70710678118654752440f;
-  // split into even/odd outputs: u = x[n] + x[n+4], w = (x[n] - x[n+4]) * W8^n
-  float2 u0 = cadd(x[0], x[4]), w0 = csub(x[0], x[4]);
-  float2 u1 = cadd(x[1], x[5]), w1 = csub(x[1], x[5]);
-  float2 u2 = cadd(x[2], x[6]), w2 = csub(x[2], x[6]);
-  float2 u3 = cadd(x[3], x[7]), w3 = csub(x[3], x[7]);
-  // W8^1 = (1 -/+ i)/sqrt2, W8^2 = -/+ i, W8^3 = (-1 -/+ i)/sqrt2
-  if (INV) {
-    w1 = make_float2((w1.x - w1.y) * r, (w1.x + w1.y) * r);
-    w3 = make_float2((-w3.x - w3.y) * r, (w3.x - w3.y) * r);
-  } else {
-    w1 = make_float2((w1.x + w1.y) * r, (w1.y - w1.x) * r);
-    w3 = make_float2((w3.y - w3.x) * r, (-w3.x - w3.y) * r);
+  float2 u[4], w[4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    u[n] = cadd(x[n], x[n + 4]);
+    w[n] = csub(x[n], x[n + 4]);
   }
-  w2 = mul_mi<INV>(w2);
-  dft4<INV>(u0, u1, u2, u3);
-  dft4<INV>(w0, w1, w2, w3);
-  x[0] = u0; x[2] = u1; x[4] = u2; x[6] = u3;
-  x[1] = w0; x[3] = w1; x[5] = w2; x[7] = w3;
+  w[1] = twiddle_const<1, 8, INV>(w[1]);
+  w[2] = twiddle_const<2, 8, INV>(w[2]);
+  w[3] = twiddle_const<3, 8, INV>(w[3]);
+  dft4<INV>(u);
+  dft4<INV>(w);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    x[2 * k] = u[k];
+    x[2 * k + 1] = w[k];
+  }
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_r(float2* x);
+
+template <int I>
+struct IntC {
+  static constexpr int value = I;
+};
+template <int I, int END, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < END) {
+    f(IntC<I>{});
+    static_for<I + 1, END>(f);
+  }
+}
+
+// Cooley-Tukey split R = A * B: n = n1 + A n2, X[k2 + B k1] = sum_n1 W_A^{n1 k1} W_R^{n1 k2} DFT_B(x[n1 + A .])[k2]
+template <int A, int B, bool INV>
+__device__ __forceinline__ void dft_split(float2* x) {
+  float2 y[A][B];
+  static_for<0, A>([&](auto n1c) {
+    constexpr int n1 = decltype(n1c)::value;
+    float2 z[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) z[n2] = x[n1 + A * n2];
+    dft_r<B, INV>(z);
+    static_for<0, B>([&](auto k2c) {
+      constexpr int k2 = decltype(k2c)::value;
+      y[n1][k2] = twiddle_const<n1 * k2, A * B, INV>(z[k2]);
+    });
+  });
+#pragma unroll
+  for (int k2 = 0; k2 < B; ++k2) {
+    float2 w[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; ++n1) w[n1] = y[n1][k2];
+    dft_r<A, INV>(w);
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) x[k2 + B * k1] = w[k1];
+  }
 }
 
 template <int R, bool INV>
 __device__ __forceinline__ void dft_r(float2* x) {
-  if (R == 8) dft8<INV>(x);
-  else if (R == 4) dft4<INV>(x[0], x[1], x[2], x[3]);
-  else dft2<INV>(x[0], x[1]);
+  if constexpr (R == 2) dft2<INV>(x);
+  else if constexpr (R == 4) dft4<INV>(x);
+  else if constexpr (R == 8) dft8<INV>(x);
+  else if constexpr (R == 16) dft_split<4, 4, INV>(x);
+  else if constexpr (R == 32) dft_split<8, 4, INV>(x);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Stage bookkeeping
+// Plans
 // ---------------------------------------------------------------------------------------------
 template <int N>
+struct Plan;
+template <> struct Plan<64> { static constexpr int P = 8, S = 2; static constexpr int R[3] = {8, 8, 1}; };
+template <> struct Plan<128> { static constexpr int P = 16, S = 2; static constexpr int R[3] = {16, 8, 1}; };
+template <> struct Plan<256> { static constexpr int P = 16, S = 2; static constexpr int R[3] = {16, 16, 1}; };
+template <> struct Plan<512> { static constexpr int P = 32, S = 2; static constexpr int R[3] = {32, 16, 1}; };
+template <> struct Plan<1024> { static constexpr int P = 32, S = 2; static constexpr int R[3] = {32, 32, 1}; };
+template <> struct Plan<2048> { static constexpr int P = 32, S = 3; static constexpr int R[3] = {32, 8, 8}; };
+template <> struct Plan<4096> { static constexpr int P = 32, S = 3; static constexpr int R[3] = {32, 16, 8}; };
+
+template <int N>
 struct Fft {
-  static_assert(N >= 64 && N <= 4096 && (N & (N - 1)) == 0, "N must be a power of two in [64, 4096]");
-  static constexpr int T = N / 8;
-  static constexpr int log2N = (N == 64) ? 6 : (N == 128) ? 7 : (N == 256) ? 8 : (N == 512) ? 9
-                             : (N == 1024) ? 10 : (N == 2048) ? 11 : 12;
-  static constexpr int n8 = log2N / 3;                 // radix-8 stages
-  static constexpr int tail = 1 << (log2N - 3 * n8);   // 1, 2 or 4
-  static constexpr int stages = n8 + (tail > 1 ? 1 : 0);
+  static constexpr int P = Plan<N>::P;
+  static constexpr int T = N / P;
+  static constexpr int stages = Plan<N>::S;
+  static constexpr int R0 = Plan<N>::R[0];
+  static constexpr int log2R0 = (R0 == 8) ? 3 : (R0 == 16) ? 4 : 5;
+  // twiddle-table size: sum over stages s >= 1 of Ns * (R_s - 1)
+  static constexpr int tw_size = (stages == 2) ? R0 * (Plan<N>::R[1] - 1)
+                                               : R0 * (Plan<N>::R[1] - 1) + R0 * Plan<N>::R[1] * (Plan<N>::R[2] - 1);
 };
 
 template <int N, int S>
 struct StageInfo {
-  static constexpr int R = (S < Fft<N>::n8) ? 8 : Fft<N>::tail;
+  static constexpr int R = Plan<N>::R[S];
   static constexpr int Ns = (S == 0) ? 1 : StageInfo<N, S - 1>::Ns * StageInfo<N, S - 1>::R;
+  static constexpr int tw_off =
+      (S <= 1) ? 0 : StageInfo<N, S - 1>::tw_off + StageInfo<N, S - 1>::Ns * (StageInfo<N, S - 1>::R - 1);
 };
 template <int N>
 struct StageInfo<N, -1> {
-  static constexpr int R = 1;
-  static constexpr int Ns = 1;
+  static constexpr int R = 1, Ns = 1, tw_off = 0;
 };
 
-// Layout functors: map (fft index g, element position n) to a float2 offset in shared memory.
-// RowLayout: each FFT owns a contiguous padded region (one pad slot every 16 elements).
+// ---------------------------------------------------------------------------------------------
+// Shared-memory address maps (float2 units) for transform g's element p
+// ---------------------------------------------------------------------------------------------
+// Contiguous per-transform regions (row pass, builder rows).
 template <int N>
 struct RowLayout {
-  static constexpr int stride = N + N / 16;
-  __device__ __forceinline__ int operator()(int g, int n) const { return g * stride + n + (n >> 4); }
+  static constexpr bool pad = (Fft<N>::T < 16);
+  static constexpr int stride = pad ? N + N / 16 : N;
+  __device__ __forceinline__ int operator()(int g, int p) const {
+    if constexpr (pad) return g * stride + p + (p >> 4);
+    else return g * stride + (p ^ ((p >> Fft<N>::log2R0) & 15));
+  }
   static constexpr int size(int G) { return G * stride; }
 };
-// ColLayout: G transforms interleaved element by element (position n of transform g at n*G+g),
-// plus one pad slot every 16 float2 when G < 8.
+// G transforms interleaved element by element (column pass): p*G + g with a one-bit swizzle.
 template <int N, int G>
 struct ColLayout {
-  __device__ __forceinline__ int operator()(int g, int n) const {
-    int o = n * G + g;
-    return (G >= 8) ? o : o + (o >> 4);
-  }
-  static constexpr int size(int) { return (G >= 8) ? N * G : N * G + (N * G) / 16 + 1; }
+  __device__ __forceinline__ int operator()(int g, int p) const { return (p ^ ((p >> Fft<N>::log2R0) & 1)) * G + g; }
+  static constexpr int size(int) { return N * G; }
 };
 
-// One Stockham stage on registers + shared memory.
-//   v: registers, layout for this stage: v[q*R + r] = element (j + q*T) + r*N/R (stage input).
-//   On return (unless LAST) v holds the inputs of stage S+1 in that stage's layout.
-template <int N, int S, bool INV, class Layout>
-__device__ __forceinline__ void stockham_stage(float2 (&v)[8], int j, int g, const float2* __restrict__ tw,
-                                               float2* sm, const Layout& L) {
-  constexpr int R = StageInfo<N, S>::R;
-  constexpr int Ns = StageInfo<N, S>::Ns;
-  constexpr int T = Fft<N>::T;
-  constexpr int Q = 8 / R;
-  constexpr bool LAST = (S == Fft<N>::stages - 1);
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int b = j + q * T;
-    if (Ns > 1) {
-      const int k = b % Ns;
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        const float2 w = tw[(k * r) * (N / (Ns * R))];
-        v[q * R + r] = INV ? cmulc(v[q * R + r], w) : cmul(v[q * R + r], w);
-      }
-    }
-    dft_r<R, INV>(&v[q * R]);
-  }
-  if (LAST) {
-    // outputs at b + r*N/R = j + T*(q + r*Q): renumber to v[m] = element j + m*T
-    if (Q > 1) {
-      float2 t[8];
+// Barrier over the threads that share one transform.
+struct SyncWarp {  // transform groups never straddle a warp
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+struct SyncBlock {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+template <int NT>
+struct SyncNamed {  // one named barrier per group of NT threads (NT a multiple of 32)
+  int id;
+  __device__ __forceinline__ void operator()() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(NT) : "memory"); }
+};
+
+// ---------------------------------------------------------------------------------------------
+// One Stockham stage.  Register layout at stage input: v[q*R + r] = x[(j + q*T) + r*N/R];
+// for stage 0 that is the entry layout v[m] = x[j + m*T] permuted at compile time.
+// ---------------------------------------------------------------------------------------------
+template <int N, int S, bool INV, class Layout, class Sync, class Hook>
+struct StageLoop {
+  __device__ __forceinline__ static void run(float2 (&v)[Fft<N>::P], int j, int g, const float2* __restrict__ tw,
+                                             float2* sm, const Layout& L, const Sync& sync, Hook& hook) {
+    constexpr int P = Fft<N>::P, T = Fft<N>::T;
+    constexpr int R = StageInfo<N, S>::R, Ns = StageInfo<N, S>::Ns;
+    constexpr int Q = P / R;
+    constexpr bool LAST = (S == Fft<N>::stages - 1);
+    if constexpr (S == 0 && Q > 1) {
+      // entry layout v[m], m = q + r*Q  ->  stage layout v[q*R + r]
+      float2 t[P];
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
-        for (int r = 0; r < R; ++r) t[q + r * Q] = v[q * R + r];
+        for (int r = 0; r < R; ++r) t[q * R + r] = v[q + r * Q];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[m] = t[m];
+      for (int m = 0; m < P; ++m) v[m] = t[m];
     }
-  } else {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const int b = j + q * T;
-      const int idxD = (b / Ns) * Ns * R + (b % Ns);
+      if constexpr (Ns > 1) {
+        const int k = b % Ns;
+        const float2* twr = tw + StageInfo<N, S>::tw_off + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sm[L(g, idxD + r * Ns)] = v[q * R + r];
+        for (int r = 1; r < R; ++r) {
+          const float2 w = twr[(r - 1) * Ns];
+          v[q * R + r] = INV ? cmulc(v[q * R + r], w) : cmul(v[q * R + r], w);
+        }
+      }
+      dft_r<R, INV>(&v[q * R]);
     }
-    __syncthreads();
-    constexpr int Rn = StageInfo<N, S + 1>::R;
-    constexpr int Qn = 8 / Rn;
+    if constexpr (LAST) {
+      // outputs at b + r*N/R = j + T*(q + r*Q): back to v[m] = x[j + m*T]
+      if constexpr (Q > 1) {
+        float2 t[P];
 #pragma unroll
-    for (int q = 0; q < Qn; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
-      for (int r = 0; r < Rn; ++r) v[q * Rn + r] = sm[L(g, j + q * T + r * (N / Rn))];
-    __syncthreads();
-  }
-}
-
-template <int N, int S, bool INV, class Layout>
-struct StageLoop {
-  __device__ __forceinline__ static void run(float2 (&v)[8], int j, int g, const float2* tw, float2* sm,
-                                             const Layout& L) {
-    stockham_stage<N, S, INV, Layout>(v, j, g, tw, sm, L);
-    StageLoop<N, S + 1, INV, Layout>::run(v, j, g, tw, sm, L);
+          for (int r = 0; r < R; ++r) t[q + r * Q] = v[q * R + r];
+#pragma unroll
+        for (int m = 0; m < P; ++m) v[m] = t[m];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int b = j + q * T;
+        const int idxD = (b / Ns) * Ns * R + (b % Ns);
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[L(g, idxD + r * Ns)] = v[q * R + r];
+      }
+      sync();
+      constexpr int Rn = StageInfo<N, S + 1>::R;
+      constexpr int Qn = P / Rn;
+#pragma unroll
+      for (int q = 0; q < Qn; ++q)
+#pragma unroll
+        for (int r = 0; r < Rn; ++r) v[q * Rn + r] = sm[L(g, j + q * T + r * (N / Rn))];
+      sync();  // the region is free for the next exchange
+      if constexpr (S + 2 == Fft<N>::stages) hook();  // last exchange done: the region is free
+      StageLoop<N, S + 1, INV, Layout, Sync, Hook>::run(v, j, g, tw, sm, L, sync, hook);
+    }
   }
 };
-template <int N, bool INV, class Layout>
-struct StageLoop<N, Fft<N>::stages, INV, Layout> {
-  __device__ __forceinline__ static void run(float2 (&)[8], int, int, const float2*, float2*, const Layout&) {}
+
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
 };
 
-// Unnormalised transform of one length-N sequence held as v[m] = x[j + m*T].
-// All threads of the CTA must call it (it contains __syncthreads()).
-template <int N, bool INV, class Layout>
-__device__ __forceinline__ void fft_regs(float2 (&v)[8], int j, int g, const float2* tw, float2* sm,
-                                         const Layout& L) {
-  StageLoop<N, 0, INV, Layout>::run(v, j, g, tw, sm, L);
+// Unnormalised transform of one length-N sequence held as v[m] = x[j + m*T].  Every thread of
+// the transform group must call it (it synchronises through ``sync``).  ``hook()`` runs once,
+// right after the last shared-memory exchange, when this transform's region is no longer read
+// by the transform (used to prefetch the next operand into it).
+template <int N, bool INV, class Layout, class Sync, class Hook = NoHook>
+__device__ __forceinline__ void fft_regs(float2 (&v)[Fft<N>::P], int j, int g, const float2* tw, float2* sm,
+                                         const Layout& L, const Sync& sync, Hook&& hook = Hook()) {
+  StageLoop<N, 0, INV, Layout, Sync, std::remove_reference_t<Hook>>::run(v, j, g, tw, sm, L, sync, hook);
 }
 
-// Cooperative copy of the twiddle table (N entries) into shared memory.
+// 8-byte asynchronous global -> shared copies (each thread later reads only what it copied).
+__device__ __forceinline__ void cp_async8(float2* smem_dst, const float2* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Launch shapes shared by the kernels that transform whole rows or whole columns.
+// Rows: G transforms of T threads per CTA (each transform inside one warp, or a named barrier
+// per transform when T > 32), at most 32 KB of exchange space per CTA.
+template <int N>
+struct RowCfg {
+  static constexpr int P = Fft<N>::P, T = Fft<N>::T;
+  static constexpr int G = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
+  // resident CTAs requested from the compiler: caps registers at 128 per thread
+  static constexpr int MINB = (512 / (G * T) > 0) ? 512 / (G * T) : 1;
+};
+// Columns: G adjacent columns per CTA, thread (j, g) = (tid / G, tid % G), so a warp's loads
+// cover 32 / G rows x G columns.
+template <int N>
+struct ColCfg {
+  static constexpr int P = Fft<N>::P, T = Fft<N>::T;
+  static constexpr int G = (N <= 1024) ? 8 : (N <= 2048 ? 4 : 2);
+  static constexpr int MINB = (512 / (G * T) > 0) ? 512 / (G * T) : 1;
+};
+
+template <int N>
+__device__ __forceinline__ auto group_sync(int g) {
+  if constexpr (Fft<N>::T <= 32) return SyncWarp{};
+  else return SyncNamed<Fft<N>::T>{1 + g};
+}
+
+// Cooperative copy of the twiddle tables into shared memory (caller synchronises afterwards).
 template <int N>
 __device__ __forceinline__ void load_twiddles(float2* dst, const float2* __restrict__ src) {
-  for (int i = threadIdx.x; i < N; i += blockDim.x) dst[i] = src[i];
+  for (int i = threadIdx.x; i < Fft<N>::tw_size; i += blockDim.x) dst[i] = src[i];
 }
 
 }  // namespace totem

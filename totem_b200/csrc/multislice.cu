@@ -14,6 +14,9 @@
 // Layout in HBM: psi[item][row][col] complex64, item = w * depth + pos (probe-major, as the
 // reference's w_series loop); T[slice][P_H][P_W]; H[N][N] and the masks [A][N][N] in natural
 // FFT order (the masks for the exit detector are ifftshift(aper), computed at upload).
+#include <cmath>
+#include <vector>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -21,23 +24,13 @@ namespace totem {
 
 namespace {
 
-template <int N>
-struct RowCfg {
-  static constexpr int T = N / 8;
-  static constexpr int G = (T >= 256) ? 1 : 256 / T;  // rows per CTA
-};
-template <int N>
-struct ColCfg {
-  static constexpr int T = N / 8;
-  static constexpr int G = (N <= 512) ? 8 : 4;        // columns per CTA
-};
-
-template <int N, int G, bool FIRST>
-__global__ void __launch_bounds__(G * (N / 8)) k_row_pass(SliceLoopArgs a, const float2* __restrict__ tslice, float scale) {
+template <int N, bool FIRST>
+__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) k_row_pass(SliceLoopArgs a, const float2* __restrict__ tslice,
+                                                                         float scale) {
+  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T, G = RowCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
-  float2* s_x = sh + N;
-  constexpr int T = N / 8;
+  float2* s_x = sh + Fft<N>::tw_size;
   const int g = threadIdx.x / T, j = threadIdx.x - g * T;
   const long grow = (long)blockIdx.x * G + g;
   const int item = (int)(grow / N), row = (int)(grow % N);
@@ -48,23 +41,36 @@ __global__ void __launch_bounds__(G * (N / 8)) k_row_pass(SliceLoopArgs a, const
   const int y0 = a.geo.begin_col + (pos % a.geo.width_red) * a.geo.step;
   const float2* __restrict__ trow = tslice + (long)x0 * a.geo.p_width + y0;
   float2* prow = a.psi + ((long)item * N + row) * N;
-  float2 v[8];
+  const RowLayout<N> L;
+  const auto sync = group_sync<N>(g);
+  // The transmission window row is copied asynchronously into this row's exchange region as soon
+  // as the region is free (kernel start for the first pass, after the inverse transform's last
+  // exchange otherwise), so its latency overlaps the transform.  Each thread copies and later
+  // reads only its own elements.
+  auto prefetch_t = [&]() {
+#pragma unroll
+    for (int m = 0; m < P; ++m) cp_async8(&s_x[L(g, j + m * T)], trow + j + m * T);
+    cp_async_commit();
+  };
+  float2 v[P];
   if (FIRST) {
+    prefetch_t();
     const float2* src = a.probe + ((long)w * N + row) * N;
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = __ldg(src + j + m * T);
+    for (int m = 0; m < P; ++m) v[m] = __ldg(src + j + m * T);
   } else {
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = prow[j + m * T];
+    for (int m = 0; m < P; ++m) v[m] = prow[j + m * T];
   }
-  __syncthreads();
-  const RowLayout<N> L;
-  if (!FIRST) fft_regs<N, true>(v, j, g, s_tw, s_x, L);
+  __syncthreads();  // twiddles staged
+  if (!FIRST) fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync, prefetch_t);
+  cp_async_wait_all();
 #pragma unroll
-  for (int m = 0; m < 8; ++m) v[m] = cscale(cmul(v[m], __ldg(trow + j + m * T)), scale);
-  fft_regs<N, false>(v, j, g, s_tw, s_x, L);
+  for (int m = 0; m < P; ++m) v[m] = cscale(cmul(v[m], s_x[L(g, j + m * T)]), scale);
+  sync();  // every thread of the transform has read its window values before the region is reused
+  fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
-  for (int m = 0; m < 8; ++m) prow[j + m * T] = v[m];
+  for (int m = 0; m < P; ++m) prow[j + m * T] = v[m];
 }
 
 // Deterministic block sum of one double per thread; result valid in thread 0.
@@ -83,53 +89,54 @@ __device__ __forceinline__ double block_sum(double x, double* red) {
   return s;
 }
 
-template <int N, int G>
-__device__ __forceinline__ void detect(const float (&inten)[8], const float* __restrict__ masks, int aper_num,
+template <int N>
+__device__ __forceinline__ void detect(const float (&inten)[Fft<N>::P], const float* __restrict__ masks, int aper_num,
                                        int j, int c, double* __restrict__ part, int item, int cb, int nblk,
                                        double* red) {
-  constexpr int T = N / 8;
+  constexpr int P = Fft<N>::P, T = Fft<N>::T;
   for (int a = 0; a < aper_num; ++a) {
     const float* mk = masks + (long)a * N * N + c;
     double acc = 0.0;
 #pragma unroll
-    for (int m = 0; m < 8; ++m) acc += (double)inten[m] * (double)__ldg(mk + (long)(j + m * T) * N);
+    for (int m = 0; m < P; ++m) acc += (double)inten[m] * (double)__ldg(mk + (long)(j + m * T) * N);
     const double s = block_sum(acc, red);
     if (threadIdx.x == 0) part[((long)item * aper_num + a) * nblk + cb] = s;
   }
 }
 
-template <int N, int G>
-__global__ void __launch_bounds__(G * (N / 8)) k_col_pass(SliceLoopArgs a, int flags) {
+template <int N>
+__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) k_col_pass(SliceLoopArgs a, int flags) {
+  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
-  float2* s_x = sh + N;
+  float2* s_x = sh + Fft<N>::tw_size;
   __shared__ double red[32];
-  constexpr int T = N / 8;
   constexpr int nblk = N / G;
   const int j = threadIdx.x / G, g = threadIdx.x - j * G;
   const int item = blockIdx.x / nblk, cb = blockIdx.x - item * nblk;
   const int c = cb * G + g;
   load_twiddles<N>(s_tw, a.tw);
   float2* base = a.psi + (long)item * N * N + c;
-  float2 v[8];
+  float2 v[P];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) v[m] = base[(long)(j + m * T) * N];
+  for (int m = 0; m < P; ++m) v[m] = base[(long)(j + m * T) * N];
   __syncthreads();
   const ColLayout<N, G> L;
-  fft_regs<N, false>(v, j, g, s_tw, s_x, L);
+  const SyncBlock sync;
+  fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
-  for (int m = 0; m < 8; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
+  for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
   if (flags & 3) {
-    float inten[8];
+    float inten[P];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) inten[m] = fmaf(v[m].x, v[m].x, v[m].y * v[m].y);
-    if (flags & 1) detect<N, G>(inten, a.mask_mid, a.aper_num, j, c, a.part_mid, item, cb, nblk, red);
-    if (flags & 2) detect<N, G>(inten, a.mask_exit, a.aper_num, j, c, a.part_exit, item, cb, nblk, red);
+    for (int m = 0; m < P; ++m) inten[m] = fmaf(v[m].x, v[m].x, v[m].y * v[m].y);
+    if (flags & 1) detect<N>(inten, a.mask_mid, a.aper_num, j, c, a.part_mid, item, cb, nblk, red);
+    if (flags & 2) detect<N>(inten, a.mask_exit, a.aper_num, j, c, a.part_exit, item, cb, nblk, red);
   }
   if (flags & 4) return;
-  fft_regs<N, true>(v, j, g, s_tw, s_x, L);
+  fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
-  for (int m = 0; m < 8; ++m) base[(long)(j + m * T) * N] = v[m];
+  for (int m = 0; m < P; ++m) base[(long)(j + m * T) * N] = v[m];
 }
 
 __global__ void k_det_reduce(const double* __restrict__ part, int nblk, int aper_num, int items, int item0,
@@ -157,24 +164,60 @@ __global__ void k_combine(const double* __restrict__ acc, const double* __restri
 template <int N, bool FIRST>
 Status row_pass(const SliceLoopArgs& a, const float2* tslice, cudaStream_t st) {
   constexpr int G = RowCfg<N>::G, T = RowCfg<N>::T;
-  const size_t smem = sizeof(float2) * (N + RowLayout<N>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_row_pass<N, G, FIRST>, smem));
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_row_pass<N, FIRST>, smem));
   const long rows = (long)a.items * N;
   const float scale = FIRST ? 1.f : 1.f / ((float)N * (float)N);
-  k_row_pass<N, G, FIRST><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale);
+  k_row_pass<N, FIRST><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale);
   return cuda_status(cudaGetLastError(), "k_row_pass");
 }
 
 template <int N>
 Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
-  const size_t smem = sizeof(float2) * (N + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, G>, smem));
-  k_col_pass<N, G><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N>, smem));
+  k_col_pass<N><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
   return cuda_status(cudaGetLastError(), "k_col_pass");
 }
 
+template <int N, int S>
+void fill_stage(std::vector<float2>& out) {
+  if constexpr (S < Fft<N>::stages) {
+    constexpr int R = StageInfo<N, S>::R, Ns = StageInfo<N, S>::Ns;
+    if constexpr (S >= 1) {
+      for (int r = 1; r < R; ++r)
+        for (int k = 0; k < Ns; ++k) {
+          const long e = (long)k * r * (N / (Ns * R));
+          const double ang = -2.0 * kPi * (double)e / (double)N;
+          out[StageInfo<N, S>::tw_off + (r - 1) * Ns + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+    }
+    fill_stage<N, S + 1>(out);
+  }
+}
+
+template <int N>
+std::vector<float2> tables() {
+  std::vector<float2> t(Fft<N>::tw_size > 0 ? Fft<N>::tw_size : 1);
+  fill_stage<N, 0>(t);
+  return t;
+}
+
 }  // namespace
+
+std::vector<float2> stage_twiddles(int n) {
+  switch (n) {
+    case 64: return tables<64>();
+    case 128: return tables<128>();
+    case 256: return tables<256>();
+    case 512: return tables<512>();
+    case 1024: return tables<1024>();
+    case 2048: return tables<2048>();
+    case 4096: return tables<4096>();
+  }
+  return {};
+}
 
 int col_blocks(int n) {
   switch (n) {

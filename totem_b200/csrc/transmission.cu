@@ -169,47 +169,48 @@ __global__ void __launch_bounds__(256) k_tx_structure(TxGrid g, AtomRowsDev nr, 
   }
 }
 
-// In-place inverse FFT of rows of length N (N/8 threads per row, G rows per CTA).
-template <int N, int G>
-__global__ void __launch_bounds__(G * (N / 8)) k_fft_rows_inv(float2* __restrict__ data, const float2* __restrict__ tw) {
+// In-place inverse FFT of rows of length N (RowCfg<N>::G rows per CTA).
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) k_fft_rows_inv(float2* __restrict__ data,
+                                                                             const float2* __restrict__ tw) {
+  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T, G = RowCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
-  float2* s_x = sh + N;
-  constexpr int T = N / 8;
+  float2* s_x = sh + Fft<N>::tw_size;
   const int g = threadIdx.x / T, j = threadIdx.x - g * T;
   const long row = (long)blockIdx.x * G + g;
   load_twiddles<N>(s_tw, tw);
   float2* p = data + row * N;
-  float2 v[8];
+  float2 v[P];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) v[m] = p[j + m * T];
+  for (int m = 0; m < P; ++m) v[m] = p[j + m * T];
   __syncthreads();
-  fft_regs<N, true>(v, j, g, s_tw, s_x, RowLayout<N>());
+  fft_regs<N, true>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
 #pragma unroll
-  for (int m = 0; m < 8; ++m) p[j + m * T] = v[m];
+  for (int m = 0; m < P; ++m) p[j + m * T] = v[m];
 }
 
 // Column inverse FFT of length N over a p_w-wide plane, (-1)^(r+c), exp(i s V).
-template <int N, int G>
-__global__ void __launch_bounds__(G * (N / 8)) k_fft_cols_exp(float2* __restrict__ data, int p_w,
-                                                             const float2* __restrict__ tw, float sig) {
+template <int N>
+__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) k_fft_cols_exp(float2* __restrict__ data, int p_w,
+                                                                             const float2* __restrict__ tw, float sig) {
+  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
-  float2* s_x = sh + N;
-  constexpr int T = N / 8;
+  float2* s_x = sh + Fft<N>::tw_size;
   const int j = threadIdx.x / G, g = threadIdx.x - j * G;
   const int nblk = p_w / G;
   const int slice = blockIdx.x / nblk, cb = blockIdx.x - slice * nblk;
   const int c = cb * G + g;
   load_twiddles<N>(s_tw, tw);
   float2* p = data + (long)slice * N * p_w + c;
-  float2 v[8];
+  float2 v[P];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) v[m] = p[(long)(j + m * T) * p_w];
+  for (int m = 0; m < P; ++m) v[m] = p[(long)(j + m * T) * p_w];
   __syncthreads();
-  fft_regs<N, true>(v, j, g, s_tw, s_x, ColLayout<N, G>());
+  fft_regs<N, true>(v, j, g, s_tw, s_x, ColLayout<N, G>(), SyncBlock());
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < P; ++m) {
     const int r = j + m * T;
     const float sgn = ((r + c) & 1) ? -1.f : 1.f;
     const float re = sgn * v[m].x * sig, im = sgn * v[m].y * sig;
@@ -239,22 +240,21 @@ __global__ void k_sign_exp(float2* __restrict__ data, long total, int p_h, int p
 
 template <int N>
 Status rows_inv(float2* data, long nrows, const float2* tw, cudaStream_t st) {
-  constexpr int T = N / 8;
-  constexpr int G = (T >= 256) ? 1 : 256 / T;
-  const size_t smem = sizeof(float2) * (N + RowLayout<N>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_fft_rows_inv<N, G>, smem));
-  k_fft_rows_inv<N, G><<<(unsigned)(nrows / G), G * T, smem, st>>>(data, tw);
+  constexpr int T = RowCfg<N>::T, G = RowCfg<N>::G;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_fft_rows_inv<N>, smem));
+  if (nrows % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "row count not a multiple of the row tile");
+  k_fft_rows_inv<N><<<(unsigned)(nrows / G), G * T, smem, st>>>(data, tw);
   return cuda_status(cudaGetLastError(), "k_fft_rows_inv");
 }
 
 template <int N>
 Status cols_exp(float2* data, int slices, int p_w, const float2* tw, float sig, cudaStream_t st) {
-  constexpr int T = N / 8;
-  constexpr int G = (N <= 512) ? 8 : (N <= 2048 ? 4 : 2);
-  const size_t smem = sizeof(float2) * (N + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_fft_cols_exp<N, G>, smem));
+  constexpr int T = ColCfg<N>::T, G = ColCfg<N>::G;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_fft_cols_exp<N>, smem));
   if (p_w % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "potential width not a multiple of the column tile");
-  k_fft_cols_exp<N, G><<<(unsigned)((long)slices * (p_w / G)), G * T, smem, st>>>(data, p_w, tw, sig);
+  k_fft_cols_exp<N><<<(unsigned)((long)slices * (p_w / G)), G * T, smem, st>>>(data, p_w, tw, sig);
   return cuda_status(cudaGetLastError(), "k_fft_cols_exp");
 }
 

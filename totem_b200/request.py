@@ -176,11 +176,14 @@ def build_srtio3_stem(cells=(8, 8, 50), n: int = 512, sampling: float = 0.0625, 
 def build_small_stem(n: int = 64, p: int = 128, raster=(3, 4), step: int = 5, slices: int = 6,
                      flag: str = PENG, kv: float = 200.0, sampling: float = 0.2,
                      detectors=((40.0, 150.0), (0.0, 15.0), (15.0, 40.0)), mid_layer=(2, 4),
-                     focal_steps: int = 1, begin=None, seed: int = 0) -> StemRequest:
-    """A small SrTiO3 case the FP64 oracle finishes in seconds (used by the parity tests)."""
+                     focal_steps: int = 1, begin=None, seed: int = 0, cells: Optional[int] = None) -> StemRequest:
+    """A small SrTiO3 case the FP64 oracle finishes in seconds (used by the parity tests).
+
+    ``cells`` limits the crystal to ``cells x cells`` unit cells (default: fill the field).
+    """
     a = 3.905
     field = p * sampling
-    ncell = max(1, int(field // a) - 1)
+    ncell = max(1, int(field // a) - 1) if cells is None else cells
     st = specimen.srtio3_001(ncell, ncell, max(1, slices // 2))
     st = specimen.center_in_field(st, field, field)
     st = specimen.Structure(st.atoms, st.extent, st.slice_dz, slices)
