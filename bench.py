@@ -33,10 +33,12 @@ sys.path.insert(0, ROOT)
 BYTES_PER_ELEM = 8  # complex64
 
 
-def build_workload(name: str, seed: int | None = None):
+def build_workload(name: str, seed: int | None = None, raster: int = 64):
     from totem_b200 import request
     if name == "stem-adf":
-        return request.build_srtio3_stem(phonon_seed=seed)
+        # a smaller raster keeps every per-probe cost identical (same window, potential, slices);
+        # it is used to time slow comparators on a subset of the 64 x 64 probes
+        return request.build_srtio3_stem(phonon_seed=seed, raster=(raster, raster), p=1024)
     if name == "stem-adf-small":
         return request.build_srtio3_stem(cells=(4, 4, 10), n=256, raster=(32, 32), sampling=0.0625, step=8)
     raise SystemExit(f"unknown workload {name}")
@@ -178,7 +180,7 @@ def run_reference(ns):
     if rank != 0:
         return
     from oracle import stem_oracle as so
-    req = build_workload(ns.workload)
+    req = build_workload(ns.workload, raster=ns.raster)
     workers = so.cpu_count()
     for _ in range(ns.warmup):
         cpu_sample(req, workers, sample_slices=1)
@@ -219,6 +221,9 @@ def main():
     ap.add_argument("--workload", default="stem-adf")
     ap.add_argument("--path", default="fused", choices=["fused", "plain"])
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--raster", type=int, default=64,
+                    help="scan positions per side (64 = the full workload; smaller only to time slow comparators)")
+    ap.add_argument("--col-variant", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ns = ap.parse_args()
@@ -238,7 +243,7 @@ def main():
         torch.cuda.set_device(local)
     from totem_b200 import capi
     path = capi.PATH_FUSED if ns.path == "fused" else capi.PATH_PLAIN
-    req = build_workload(ns.workload)
+    req = build_workload(ns.workload, raster=ns.raster)
     # a dedicated stream: the engine launches on it and the CUDA events below are recorded on it
     # (the legacy default stream has handle 0, which the C ABI reads as "make your own stream")
     stream = torch.cuda.Stream()
@@ -246,7 +251,7 @@ def main():
     sess.upload(req)
 
     def step():
-        sess.run(path=path, batch=ns.batch)
+        sess.run(path=path, batch=ns.batch, col_variant=ns.col_variant)
 
     for _ in range(max(ns.warmup, 0)):
         step()
@@ -275,7 +280,7 @@ def main():
     value = ws * units * ns.steps / (ms_total / 1000.0)
 
     # per-kernel device times (events around every pass) for the roofline
-    sess.run(path=path, batch=ns.batch, profile=True)
+    sess.run(path=path, batch=ns.batch, profile=True, col_variant=ns.col_variant)
     tm = sess.timing()
     peak, peak_kind = measured_peaks()
     n2 = req.height * req.width

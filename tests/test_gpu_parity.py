@@ -112,8 +112,8 @@ def test_session_reuse_and_batches(engine_lib):
     s = capi.Session()
     s.upload(req)
     outs = []
-    for b in (1, 3, 7, 0):
-        s.run(batch=b)
+    for b, cv in ((1, 0), (3, 1), (7, 2), (0, 2)):
+        s.run(batch=b, col_variant=cv)
         res, mid, _ = s.download()
         outs.append((res, mid))
     for r, m in outs[1:]:

@@ -47,7 +47,8 @@ class TotemStemOut(C.Structure):
 
 
 class TotemRunOptions(C.Structure):
-    _fields_ = [("path", C.c_int), ("batch", C.c_int), ("skip_transmission", C.c_int), ("profile", C.c_int)]
+    _fields_ = [("path", C.c_int), ("batch", C.c_int), ("skip_transmission", C.c_int), ("profile", C.c_int),
+                ("col_variant", C.c_int)]
 
 
 class TotemTiming(C.Structure):
@@ -212,8 +213,8 @@ class Session:
         check(self.lib.totem_session_upload(self.h, C.byref(self._m.args)))
 
     def run(self, what: int = 0, path: int = PATH_FUSED, batch: int = 0, skip_transmission: bool = False,
-            profile: bool = False):
-        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile))
+            profile: bool = False, col_variant: int = 0):
+        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile), col_variant)
         check(self.lib.totem_session_run(self.h, what, C.byref(o)))
 
     def download(self, want_transmission: bool = False):
@@ -248,7 +249,7 @@ def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
     res = np.zeros(req.aper_num * req.depth)
     mid = np.zeros(req.aper_num * req.depth * len(req.mid_layer))
     out = TotemStemOut(_ptr(res), _ptr(mid), None, None)
-    opt = TotemRunOptions(path, batch, 0, 0)
+    opt = TotemRunOptions(path, batch, 0, 0, 0)
     check(lib.totem_stem_run(C.byref(m.args), C.byref(opt), C.byref(out)))
     return res, mid
 

@@ -228,7 +228,7 @@ struct totem_session {
 
   Status upload_args(const TotemStemArgs* a, bool stem);
   Status build_transmission(int path, int* launches);
-  Status slice_loop(int path, int batch, int* launches, int* batch_used);
+  Status slice_loop(int path, int batch, int col_variant, int* launches, int* batch_used);
   Status run(int what, const TotemRunOptions* opt);
   Status collect_timing();
   Status download(TotemStemOut* out);
@@ -435,7 +435,7 @@ Status totem_session::build_transmission(int path, int* launches) {
 // ---------------------------------------------------------------------------------------------
 // Slice loop
 // ---------------------------------------------------------------------------------------------
-Status totem_session::slice_loop(int path, int batch, int* launches, int* batch_used) {
+Status totem_session::slice_loop(int path, int batch, int col_variant, int* launches, int* batch_used) {
   const long items_total = (long)w_num * depth;
   const long ad = (long)aper_num * depth;
   const int L = (int)mid_layer.size();
@@ -492,6 +492,7 @@ Status totem_session::slice_loop(int path, int batch, int* launches, int* batch_
       s.psi = psi.as<float2>(); s.probe = probe.as<float2>(); s.prop = prop.as<float2>();
       s.tw = tw_n.as<float2>(); s.aper_num = aper_num;
       s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
+      s.col_variant = (col_variant == 2) ? 1 : 0;
       TOTEM_TRY(prof_begin());
       TOTEM_TRY(totem::launch_row_pass(s, Tp, true, stream));
       TOTEM_TRY(prof_end(0));
@@ -584,7 +585,7 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
   TOTEM_CUDA(cudaEventRecord(ev[1], stream));
   if (what == 0) {
     if (!stem_ready && depth > 0) return Status::Err(TOTEM_ERR_STATE, "no STEM inputs uploaded");
-    TOTEM_TRY(slice_loop(o.path, o.batch, &launches, &batch_used));
+    TOTEM_TRY(slice_loop(o.path, o.batch, o.col_variant, &launches, &batch_used));
   }
   else has_result = true;
   TOTEM_CUDA(cudaEventRecord(ev[2], stream));

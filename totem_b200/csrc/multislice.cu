@@ -104,8 +104,12 @@ __device__ __forceinline__ void detect(const float (&inten)[Fft<N>::P], const fl
   }
 }
 
-template <int N>
-__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) k_col_pass(SliceLoopArgs a, int flags) {
+// LEAN = true: the propagator is read straight from global memory (L2) and the kernel fits in
+// fewer registers, so more CTAs are resident; LEAN = false: the propagator column is prefetched
+// into shared memory while the forward transform finishes.
+template <int N, bool LEAN>
+__global__ void __launch_bounds__(ColCfg<N, LEAN>::G * ColCfg<N, LEAN>::T, ColCfg<N, LEAN>::MINB)
+    k_col_pass(SliceLoopArgs a, int flags) {
   constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
@@ -123,9 +127,24 @@ __global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) 
   __syncthreads();
   const ColLayout<N, G> L;
   const SyncBlock sync;
-  fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
+  // the propagator column is prefetched into the exchange region once the forward transform
+  // has finished with it (each thread copies and reads only its own elements)
+  if constexpr (LEAN) {
+    fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
+    for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
+  } else {
+    auto prefetch_h = [&]() {
+#pragma unroll
+      for (int m = 0; m < P; ++m) cp_async8(&s_x[L(g, j + m * T)], a.prop + (long)(j + m * T) * N + c);
+      cp_async_commit();
+    };
+    fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync, prefetch_h);
+    cp_async_wait_all();
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m] = cmul(v[m], s_x[L(g, j + m * T)]);
+    sync();  // all propagator values read before the inverse transform reuses the region
+  }
   if (flags & 3) {
     float inten[P];
 #pragma unroll
@@ -172,13 +191,18 @@ Status row_pass(const SliceLoopArgs& a, const float2* tslice, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_row_pass");
 }
 
-template <int N>
-Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
+template <int N, bool LEAN>
+Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N>, smem));
-  k_col_pass<N><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
+  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, LEAN>, smem));
+  k_col_pass<N, LEAN><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
   return cuda_status(cudaGetLastError(), "k_col_pass");
+}
+
+template <int N>
+Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
+  return a.col_variant == 1 ? col_pass_v<N, true>(a, flags, st) : col_pass_v<N, false>(a, flags, st);
 }
 
 template <int N, int S>
