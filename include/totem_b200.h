@@ -112,8 +112,9 @@ typedef struct TotemRunOptions {
   int batch;                       /* probes in flight per batch, 0 = engine's choice          */
   int skip_transmission;           /* 1 = reuse the transmission built by an earlier run        */
   int profile;                     /* 1 = CUDA events around every slice-loop pass launch       */
-  int col_variant;                 /* fused column pass: 0 = engine default, 1 = propagator
-                                      prefetched to shared memory, 2 = lean (more resident CTAs) */
+  int col_variant;                 /* fused column pass: 0 = engine default (propagator read from
+                                      L2), 2 = propagator prefetched to shared memory, 3 = 80-register
+                                      cap (more resident CTAs)                                      */
 } TotemRunOptions;
 
 /* Device times (CUDA events) of the last run, milliseconds. */

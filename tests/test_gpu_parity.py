@@ -112,7 +112,7 @@ def test_session_reuse_and_batches(engine_lib):
     s = capi.Session()
     s.upload(req)
     outs = []
-    for b, cv in ((1, 0), (3, 1), (7, 2), (0, 2)):
+    for b, cv in ((1, 0), (3, 2), (7, 3), (0, 0)):
         s.run(batch=b, col_variant=cv)
         res, mid, _ = s.download()
         outs.append((res, mid))

@@ -111,7 +111,7 @@ struct SliceLoopArgs {
   const float* mask_exit = nullptr;
   double* part_mid = nullptr;      // [items][A][nblk]
   double* part_exit = nullptr;
-  int col_variant = 0;             // 0: propagator prefetched to shared memory, 1: lean (more CTAs)
+  int col_variant = 0;             // 0/1: default, 2: propagator prefetched, 3: 80-register cap
 };
 int col_blocks(int n);             // number of column blocks per item (partials per detector)
 Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st);

@@ -376,13 +376,11 @@ struct RowCfg {
 };
 // Columns: G adjacent columns per CTA, thread (j, g) = (tid / G, tid % G), so a warp's loads
 // cover 32 / G rows x G columns.
-template <int N, bool LEAN = false>
+template <int N, int CTAS128 = 4>
 struct ColCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
   static constexpr int G = (N <= 1024) ? 8 : (N <= 2048 ? 4 : 2);
-  // resident CTAs of 128 threads requested per SM.  The lean column pass (no propagator
-  // prefetch) fits in 80 registers up to N = 1024; the others keep the 128-register cap.
-  static constexpr int CTAS128 = (LEAN && N <= 1024) ? 6 : 4;
+  // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };
 

@@ -104,11 +104,12 @@ __device__ __forceinline__ void detect(const float (&inten)[Fft<N>::P], const fl
   }
 }
 
-// LEAN = true: the propagator is read straight from global memory (L2) and the kernel fits in
-// fewer registers, so more CTAs are resident; LEAN = false: the propagator column is prefetched
-// into shared memory while the forward transform finishes.
-template <int N, bool LEAN>
-__global__ void __launch_bounds__(ColCfg<N, LEAN>::G * ColCfg<N, LEAN>::T, ColCfg<N, LEAN>::MINB)
+// Variants (measured on the SrTiO3 512^2 workload, per 4096-probe launch): the propagator read
+// straight from global memory (L2-resident) at a 128-register cap, 4.3 ms (the default); the
+// propagator column prefetched into shared memory while the forward transform finishes, 4.6 ms;
+// the direct read at an 80-register cap (6 CTAs per SM), 5.8 ms.
+template <int N, bool PREFETCH, int CTAS128>
+__global__ void __launch_bounds__(ColCfg<N, CTAS128>::G * ColCfg<N, CTAS128>::T, ColCfg<N, CTAS128>::MINB)
     k_col_pass(SliceLoopArgs a, int flags) {
   constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
   extern __shared__ float2 sh[];
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(ColCfg<N, LEAN>::G * ColCfg<N, LEAN>::T, ColCf
   const SyncBlock sync;
   // the propagator column is prefetched into the exchange region once the forward transform
   // has finished with it (each thread copies and reads only its own elements)
-  if constexpr (LEAN) {
+  if constexpr (!PREFETCH) {
     fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
     for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
@@ -191,18 +192,22 @@ Status row_pass(const SliceLoopArgs& a, const float2* tslice, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_row_pass");
 }
 
-template <int N, bool LEAN>
+template <int N, bool PREFETCH, int CTAS128>
 Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, LEAN>, smem));
-  k_col_pass<N, LEAN><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
+  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128>, smem));
+  k_col_pass<N, PREFETCH, CTAS128><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
   return cuda_status(cudaGetLastError(), "k_col_pass");
 }
 
 template <int N>
 Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
-  return a.col_variant == 1 ? col_pass_v<N, true>(a, flags, st) : col_pass_v<N, false>(a, flags, st);
+  switch (a.col_variant) {
+    case 2: return col_pass_v<N, true, 4>(a, flags, st);
+    case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4)>(a, flags, st);
+    default: return col_pass_v<N, false, 4>(a, flags, st);
+  }
 }
 
 template <int N, int S>
