@@ -161,6 +161,37 @@ TOTEM_API int totem_stem_run(const TotemStemArgs *args, const TotemRunOptions *o
  * transmission exp(i sigma V / 1000)).  Replaces cuda_source_lobato_potential.cu:747. */
 TOTEM_API int totem_transmission_run(const TotemStemArgs *args, TotemStemOut *out);
 
+/* Size of the fixed device scratch array used by totem_stem_slices_noalloc (per GPU). */
+#define TOTEM_NOALLOC_SCRATCH_BYTES (32ull << 20)
+
+/*
+ * Slice loop and exit detectors without any device allocation.  This entry point has no
+ * counterpart in the reference; it exists for callers that cannot allocate device memory:
+ * code whose GPU memory belongs to a host framework's pool (a MEX function under MATLAB's GPU
+ * memory manager, an operator in a PyTorch pipeline that must not bypass its caching
+ * allocator), latency-bound serving loops that cannot pay for cudaMalloc / cudaFree (both
+ * synchronise the device and stall other streams), and deployments with a fixed memory budget.
+ *
+ * All pointers are device memory owned by the caller: transmission complex64
+ * [slices][p_height][p_width]; probe complex64 [w_num][n][n]; propagator complex64 [n][n] in FFT
+ * order; masks float32 [aper_num][n][n] in FFT order (ifftshift of the centred detector masks);
+ * result float64 [aper_num][items] receives sum |Psi|^2 * mask for items item0 .. item0+items-1,
+ * item = w * depth + pos, with the window of pos placed as in TotemStemArgs.  No gfsf weighting.
+ *
+ * Intermediate buffers live in one fixed device array of TOTEM_NOALLOC_SCRATCH_BYTES (32 MiB)
+ * that the library holds on every GPU that loads it until the process exits; a request that
+ * needs more (about 15 probes of 512^2 per call) fails with TOTEM_ERR_INVALID_ARG and a message
+ * (totem_last_error) giving the largest batch that fits.  The first call on a device performs a
+ * one-time set-up with that device current (the array's device address and a blocking copy of
+ * FFT twiddle tables into it); make that first call before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race; calls ordered on one stream do not.
+ * n must be a power of two in [64, 2048] and slices >= 1.  Asynchronous on ``stream``.
+ */
+TOTEM_API int totem_stem_slices_noalloc(const void *transmission, int p_height, int p_width, int slices,
+                                        const void *probe, int w_num, const void *propagator, const float *masks,
+                                        int aper_num, int n, int step, int begin_row, int begin_col, int width_red,
+                                        int depth, int item0, int items, double *result, void *stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 

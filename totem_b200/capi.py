@@ -95,9 +95,11 @@ def load() -> C.CDLL:
     lib.totem_session_transmission.argtypes = [vp, C.POINTER(vp)]
     lib.totem_stem_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemRunOptions), C.POINTER(TotemStemOut)]
     lib.totem_transmission_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemStemOut)]
+    lib.totem_stem_slices_noalloc.argtypes = ([vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp] + [C.c_int] * 9
+                                              + [vp, vp])
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
                  "totem_session_download", "totem_session_timing", "totem_session_transmission",
-                 "totem_stem_run", "totem_transmission_run"):
+                 "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -240,6 +242,23 @@ class Session:
         t = TotemTiming()
         check(self.lib.totem_session_timing(self.h, C.byref(t)))
         return t
+
+    def transmission_ptr(self) -> int:
+        """Device address of the transmission stack built by the last run (complex64)."""
+        p = C.c_void_p()
+        check(self.lib.totem_session_transmission(self.h, C.byref(p)))
+        return p.value
+
+
+def stem_slices_noalloc(transmission: int, p_height: int, p_width: int, slices: int, probe: int, w_num: int,
+                        propagator: int, masks: int, aper_num: int, n: int, step: int, begin_row: int,
+                        begin_col: int, width_red: int, depth: int, item0: int, items: int, result: int,
+                        stream: int | None = None):
+    """``totem_stem_slices_noalloc``: every pointer is a device address owned by the caller."""
+    lib = load()
+    check(lib.totem_stem_slices_noalloc(transmission, p_height, p_width, slices, probe, w_num, propagator, masks,
+                                        aper_num, n, step, begin_row, begin_col, width_red, depth, item0, items,
+                                        result, stream))
 
 
 def stem_run(req, path: int = PATH_FUSED, batch: int = 0):

@@ -28,6 +28,8 @@ Status cuda_status(cudaError_t e, const char* what);
 Status cufft_status(cufftResult r, const char* what);
 // Raise a kernel's dynamic shared-memory limit once (cached per function pointer).
 Status ensure_smem(const void* func, size_t bytes);
+// Set the calling thread's message returned by totem_last_error().
+void set_last_error(const std::string& msg);
 
 #define TOTEM_CUDA(call)                                              \
   do {                                                                \

@@ -147,6 +147,8 @@ struct PlanKey {
 
 }  // namespace
 
+void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 struct totem_session {
   int device = 0;
   cudaStream_t stream = nullptr;
