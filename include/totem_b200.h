@@ -113,8 +113,9 @@ typedef struct TotemRunOptions {
   int skip_transmission;           /* 1 = reuse the transmission built by an earlier run        */
   int profile;                     /* 1 = CUDA events around every slice-loop pass launch       */
   int col_variant;                 /* fused column pass: 0 = engine default (propagator read from
-                                      L2), 2 = propagator prefetched to shared memory, 3 = 80-register
-                                      cap (more resident CTAs)                                      */
+                                      L2, 16-column tiles up to N = 512), 2 = propagator prefetched
+                                      to shared memory, 3 = 80-register cap (more resident CTAs),
+                                      5 = 8-column tiles, 6 = 32-column tiles (N <= 512)           */
 } TotemRunOptions;
 
 /* Device times (CUDA events) of the last run, milliseconds. */

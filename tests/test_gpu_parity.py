@@ -112,7 +112,7 @@ def test_session_reuse_and_batches(engine_lib):
     s = capi.Session()
     s.upload(req)
     outs = []
-    for b, cv in ((1, 0), (3, 2), (7, 3), (0, 0)):
+    for b, cv in ((1, 0), (3, 2), (7, 3), (0, 0), (2, 1)):
         s.run(batch=b, col_variant=cv)
         res, mid, _ = s.download()
         outs.append((res, mid))
@@ -121,6 +121,12 @@ def test_session_reuse_and_batches(engine_lib):
     _check(req, *outs[0])
     t = s.timing()
     assert t.kernel_launches > 0 and t.total_ms > 0
+    # wider column tiles regroup the FP64 detector sums: equal to rounding, not bit for bit
+    for cv in (5, 6):
+        s.run(batch=5, col_variant=cv)
+        res, mid, _ = s.download()
+        np.testing.assert_allclose(res, outs[0][0], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(mid, outs[0][1], rtol=1e-12, atol=0)
     s.close()
 
 

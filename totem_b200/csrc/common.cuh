@@ -113,9 +113,10 @@ struct SliceLoopArgs {
   const float* mask_exit = nullptr;
   double* part_mid = nullptr;      // [items][A][nblk]
   double* part_exit = nullptr;
-  int col_variant = 0;             // 0/1: default, 2: propagator prefetched, 3: 80-register cap
+  int col_variant = 0;             // column-pass variant (multislice.cu, col_pass)
 };
-int col_blocks(int n);             // number of column blocks per item (partials per detector)
+// Number of column tiles per item (detector partial sums per probe) of a column-pass variant.
+int col_blocks(int n, int variant = 0);
 Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st);
 // flags: 1 = mid-slice detectors, 2 = exit detectors, 4 = final pass (no inverse transform)
 Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st);

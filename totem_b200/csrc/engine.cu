@@ -478,7 +478,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int* laun
     B = (int)((items_total + nb - 1) / nb);
   }
   *batch_used = B;
-  const int nblk = fused ? totem::col_blocks(h) : 64;
+  const int nblk = fused ? totem::col_blocks(h, col_variant) : 64;
   TOTEM_TRY(psi.ensure((size_t)B * vol * sizeof(float2)));
   TOTEM_TRY(part.ensure((size_t)n_events * B * aper_num * nblk * sizeof(double)));
   TOTEM_TRY(acc.ensure((size_t)n_events * w_num * ad * sizeof(double)));

@@ -242,22 +242,44 @@ struct StageInfo<N, -1> {
 // ---------------------------------------------------------------------------------------------
 // Shared-memory address maps (float2 units) for transform g's element p
 // ---------------------------------------------------------------------------------------------
+// Both maps pad one slot after every R0 elements (R0 = the first radix): p -> p + p / R0.  With
+// that padding every 64-bit store and load of the exchanges hits distinct banks for all plans
+// (checked by simulation of each stage's access pattern and by ncu), and because the stage
+// patterns decompose as p = lo + hi * R0 with lo < R0 known by construction, every address is a
+// per-thread base plus a compile-time offset (``split``), with no index arithmetic per element.
+template <int N>
+struct PadMap {
+  static constexpr int R0 = Fft<N>::R0;
+  __device__ __forceinline__ static int pad(int p) { return p + p / R0; }
+  __device__ __forceinline__ static int split(int hi, int lo) { return hi * (R0 + 1) + lo; }
+  // padded index of position p = j + m*T (the register layout of a thread)
+  __device__ __forceinline__ static int pos(int j, int m) {
+    constexpr int T = Fft<N>::T;
+    if constexpr (T <= R0) {
+      constexpr int per = R0 / T;  // register slots per R0 block
+      return split(m / per, j + (m % per) * T);
+    } else {
+      return split(j / R0 + m * (T / R0), j % R0);
+    }
+  }
+};
 // Contiguous per-transform regions (row pass, builder rows).
 template <int N>
 struct RowLayout {
-  static constexpr bool pad = (Fft<N>::T < 16);
-  static constexpr int stride = pad ? N + N / 16 : N;
-  __device__ __forceinline__ int operator()(int g, int p) const {
-    if constexpr (pad) return g * stride + p + (p >> 4);
-    else return g * stride + (p ^ ((p >> Fft<N>::log2R0) & 15));
-  }
+  static constexpr int stride = N + N / Fft<N>::R0;
+  __device__ __forceinline__ int operator()(int g, int p) const { return g * stride + PadMap<N>::pad(p); }
+  __device__ __forceinline__ int split(int g, int hi, int lo) const { return g * stride + PadMap<N>::split(hi, lo); }
+  __device__ __forceinline__ int pos(int g, int j, int m) const { return g * stride + PadMap<N>::pos(j, m); }
   static constexpr int size(int G) { return G * stride; }
 };
-// G transforms interleaved element by element (column pass): p*G + g with a one-bit swizzle.
+// G transforms interleaved element by element (column pass): element p of transform g at
+// pad(p) * G + g.
 template <int N, int G>
 struct ColLayout {
-  __device__ __forceinline__ int operator()(int g, int p) const { return (p ^ ((p >> Fft<N>::log2R0) & 1)) * G + g; }
-  static constexpr int size(int) { return N * G; }
+  __device__ __forceinline__ int operator()(int g, int p) const { return PadMap<N>::pad(p) * G + g; }
+  __device__ __forceinline__ int split(int g, int hi, int lo) const { return PadMap<N>::split(hi, lo) * G + g; }
+  __device__ __forceinline__ int pos(int g, int j, int m) const { return PadMap<N>::pos(j, m) * G + g; }
+  static constexpr int size(int) { return (N + N / Fft<N>::R0) * G; }
 };
 
 // Barrier over the threads that share one transform.
@@ -285,6 +307,7 @@ struct StageLoop {
     constexpr int R = StageInfo<N, S>::R, Ns = StageInfo<N, S>::Ns;
     constexpr int Q = P / R;
     constexpr bool LAST = (S == Fft<N>::stages - 1);
+    __builtin_assume(j >= 0 && j < T);
     if constexpr (S == 0 && Q > 1) {
       // entry layout v[m], m = q + r*Q  ->  stage layout v[q*R + r]
       float2 t[P];
@@ -324,9 +347,15 @@ struct StageLoop {
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int b = j + q * T;
-        const int idxD = (b / Ns) * Ns * R + (b % Ns);
+        if constexpr (S == 0) {
+          // p = R0 * b + r with r < R0
 #pragma unroll
-        for (int r = 0; r < R; ++r) sm[L(g, idxD + r * Ns)] = v[q * R + r];
+          for (int r = 0; r < R; ++r) sm[L.split(g, b, r)] = v[q * R + r];
+        } else {
+          const int idxD = (b / Ns) * Ns * R + (b % Ns);
+#pragma unroll
+          for (int r = 0; r < R; ++r) sm[L(g, idxD + r * Ns)] = v[q * R + r];
+        }
       }
       sync();
       constexpr int Rn = StageInfo<N, S + 1>::R;
@@ -334,7 +363,14 @@ struct StageLoop {
 #pragma unroll
       for (int q = 0; q < Qn; ++q)
 #pragma unroll
-        for (int r = 0; r < Rn; ++r) v[q * Rn + r] = sm[L(g, j + q * T + r * (N / Rn))];
+        for (int r = 0; r < Rn; ++r) {
+          if constexpr (N / Rn == Fft<N>::R0) {
+            // p = (j + q*T) + r * R0 with j + q*T < N / Rn = R0
+            v[q * Rn + r] = sm[L.split(g, r, j + q * T)];
+          } else {
+            v[q * Rn + r] = sm[L(g, j + q * T + r * (N / Rn))];
+          }
+        }
       sync();  // the region is free for the next exchange
       if constexpr (S + 2 == Fft<N>::stages) hook();  // last exchange done: the region is free
       StageLoop<N, S + 1, INV, Layout, Sync, Hook>::run(v, j, g, tw, sm, L, sync, hook);
@@ -371,15 +407,19 @@ template <int N>
 struct RowCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
   static constexpr int G = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
-  // resident CTAs requested from the compiler: caps registers at 128 per thread
-  static constexpr int MINB = (512 / (G * T) > 0) ? 512 / (G * T) : 1;
+  // resident CTAs of 128 threads requested per SM: 5 caps registers at 96 per thread, which
+  // the padded exchange addressing fits without spilling up to N = 1024 (and 5 CTAs is also
+  // what the row pass's shared memory allows)
+  static constexpr int CTAS128 = (N <= 1024) ? 5 : 4;
+  static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };
 // Columns: G adjacent columns per CTA, thread (j, g) = (tid / G, tid % G), so a warp's loads
 // cover 32 / G rows x G columns.
-template <int N, int CTAS128 = 4>
+template <int N, int CTAS128 = 4, int GW = 0>
 struct ColCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
-  static constexpr int G = (N <= 1024) ? 8 : (N <= 2048 ? 4 : 2);
+  // GW = 0: the default width, 16 columns (one 128-byte segment per row) up to N = 512
+  static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 1024 ? 8 : (N <= 2048 ? 4 : 2)));
   // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };

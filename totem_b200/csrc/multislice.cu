@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) 
   // reads only its own elements.
   auto prefetch_t = [&]() {
 #pragma unroll
-    for (int m = 0; m < P; ++m) cp_async8(&s_x[L(g, j + m * T)], trow + j + m * T);
+    for (int m = 0; m < P; ++m) cp_async8(&s_x[L.pos(g, j, m)], trow + j + m * T);
     cp_async_commit();
   };
   float2 v[P];
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) 
   if (!FIRST) fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync, prefetch_t);
   cp_async_wait_all();
 #pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = cscale(cmul(v[m], s_x[L(g, j + m * T)]), scale);
+  for (int m = 0; m < P; ++m) v[m] = cscale(cmul(v[m], s_x[L.pos(g, j, m)]), scale);
   sync();  // every thread of the transform has read its window values before the region is reused
   fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
@@ -108,10 +108,10 @@ __device__ __forceinline__ void detect(const float (&inten)[Fft<N>::P], const fl
 // straight from global memory (L2-resident) at a 128-register cap, 4.3 ms (the default); the
 // propagator column prefetched into shared memory while the forward transform finishes, 4.6 ms;
 // the direct read at an 80-register cap (6 CTAs per SM), 5.8 ms.
-template <int N, bool PREFETCH, int CTAS128>
-__global__ void __launch_bounds__(ColCfg<N, CTAS128>::G * ColCfg<N, CTAS128>::T, ColCfg<N, CTAS128>::MINB)
+template <int N, bool PREFETCH, int CTAS128, int GW>
+__global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
     k_col_pass(SliceLoopArgs a, int flags) {
-  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
+  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N, CTAS128, GW>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
@@ -128,8 +128,8 @@ __global__ void __launch_bounds__(ColCfg<N, CTAS128>::G * ColCfg<N, CTAS128>::T,
   __syncthreads();
   const ColLayout<N, G> L;
   const SyncBlock sync;
-  // the propagator column is prefetched into the exchange region once the forward transform
-  // has finished with it (each thread copies and reads only its own elements)
+  // PREFETCH: the propagator column is copied into the exchange region once the forward
+  // transform has finished with it (each thread copies and reads only its own elements)
   if constexpr (!PREFETCH) {
     fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
@@ -137,13 +137,13 @@ __global__ void __launch_bounds__(ColCfg<N, CTAS128>::G * ColCfg<N, CTAS128>::T,
   } else {
     auto prefetch_h = [&]() {
 #pragma unroll
-      for (int m = 0; m < P; ++m) cp_async8(&s_x[L(g, j + m * T)], a.prop + (long)(j + m * T) * N + c);
+      for (int m = 0; m < P; ++m) cp_async8(&s_x[L.pos(g, j, m)], a.prop + (long)(j + m * T) * N + c);
       cp_async_commit();
     };
     fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync, prefetch_h);
     cp_async_wait_all();
 #pragma unroll
-    for (int m = 0; m < P; ++m) v[m] = cmul(v[m], s_x[L(g, j + m * T)]);
+    for (int m = 0; m < P; ++m) v[m] = cmul(v[m], s_x[L.pos(g, j, m)]);
     sync();  // all propagator values read before the inverse transform reuses the region
   }
   if (flags & 3) {
@@ -192,22 +192,35 @@ Status row_pass(const SliceLoopArgs& a, const float2* tslice, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_row_pass");
 }
 
-template <int N, bool PREFETCH, int CTAS128>
+template <int N, bool PREFETCH, int CTAS128, int GW>
 Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
-  constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
+  constexpr int G = ColCfg<N, CTAS128, GW>::G, T = ColCfg<N>::T;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128>, smem));
-  k_col_pass<N, PREFETCH, CTAS128><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
+  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128, GW>, smem));
+  k_col_pass<N, PREFETCH, CTAS128, GW><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
   return cuda_status(cudaGetLastError(), "k_col_pass");
 }
 
+// Column-pass variants: 0/1 default; 2 propagator prefetched to shared memory; 3 a cap of
+// 6 x 128 threads per SM (80 registers at 16 columns); 5 tiles of 8 columns (up to N = 1024);
+// 6 tiles of 32 columns (up to N = 512).  col_blocks() gives the number of column tiles, i.e. of
+// detector partial sums per probe, of each variant.
 template <int N>
 Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   switch (a.col_variant) {
-    case 2: return col_pass_v<N, true, 4>(a, flags, st);
-    case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4)>(a, flags, st);
-    default: return col_pass_v<N, false, 4>(a, flags, st);
+    case 2: return col_pass_v<N, true, 4, 0>(a, flags, st);
+    case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4), 0>(a, flags, st);
+    case 5: return col_pass_v<N, false, 4, (N <= 1024 ? 8 : 0)>(a, flags, st);
+    case 6: return col_pass_v<N, false, 4, (N <= 512 ? 32 : 0)>(a, flags, st);
+    default: return col_pass_v<N, false, 4, 0>(a, flags, st);
   }
+}
+
+template <int N>
+int col_tiles(int variant) {
+  if (N <= 1024 && variant == 5) return N / 8;
+  if (N <= 512 && variant == 6) return N / 32;
+  return N / ColCfg<N>::G;
 }
 
 template <int N, int S>
@@ -248,14 +261,14 @@ std::vector<float2> stage_twiddles(int n) {
   return {};
 }
 
-int col_blocks(int n) {
+int col_blocks(int n, int variant) {
   switch (n) {
-    case 64: return 64 / ColCfg<64>::G;
-    case 128: return 128 / ColCfg<128>::G;
-    case 256: return 256 / ColCfg<256>::G;
-    case 512: return 512 / ColCfg<512>::G;
-    case 1024: return 1024 / ColCfg<1024>::G;
-    case 2048: return 2048 / ColCfg<2048>::G;
+    case 64: return col_tiles<64>(variant);
+    case 128: return col_tiles<128>(variant);
+    case 256: return col_tiles<256>(variant);
+    case 512: return col_tiles<512>(variant);
+    case 1024: return col_tiles<1024>(variant);
+    case 2048: return col_tiles<2048>(variant);
   }
   return 0;
 }
