@@ -48,7 +48,8 @@ enum {
   TOTEM_ERR_CUFFT = 4,         /* a cuFFT call failed                                 */
   TOTEM_ERR_OOM = 5,           /* device allocation failed                            */
   TOTEM_ERR_NO_DEVICE = 6,     /* no CUDA device is visible                           */
-  TOTEM_ERR_STATE = 7          /* call sequence error (e.g. run before upload)        */
+  TOTEM_ERR_STATE = 7,         /* call sequence error (e.g. run before upload)        */
+  TOTEM_ERR_TIMEOUT = 8        /* a wait ended before the request finished            */
 };
 
 /* Scattering-factor parameterisation: selects the coefficient-row layout, i.e. which MEX the
@@ -192,6 +193,83 @@ TOTEM_API int totem_stem_slices_noalloc(const void *transmission, int p_height, 
                                         const void *probe, int w_num, const void *propagator, const float *masks,
                                         int aper_num, int n, int step, int begin_row, int begin_col, int width_red,
                                         int depth, int item0, int items, double *result, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Serving: a resident scheduler with continuous batching.  No counterpart in the reference,
+ * whose entry point runs one blocking request at a time and allocates / frees everything per
+ * call (waveCuda.cpp:4-101, cuda_source_lobato.cu:1018-1562).
+ *
+ * Requests are queued by totem_server_submit and run asynchronously:
+ *   1. admission: a request waits until its resident footprint (transmission stack, probe,
+ *      propagator, masks, coefficient rows, detector sums) fits in the budget;
+ *   2. preparation (own stream, concurrent with running requests): upload and transmission build;
+ *   3. slice loop: every tick advances all running probe groups by one slice, in one row-pass and
+ *      one column-pass launch per window size.  Groups of probes from any number of requests, each
+ *      at its own slice, share those launches, so a request's probes start as soon as wave memory
+ *      is free and small requests run in the gaps of large ones;
+ *   4. completion: detector sums are combined and copied into the caller's TotemStemOut buffers.
+ * Results are bit-identical to totem_stem_run on the same request (same kernels, same fixed
+ * summation order), whatever else runs at the same time.
+ *
+ * The caller keeps every buffer of ``args`` and ``out`` alive and unmodified until the request is
+ * done (totem_server_wait returned or totem_server_info reports DONE / FAILED).  Only the fused
+ * path is served: the window must be square, a power of two in [64, 2048], and slices >= 1.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct totem_server totem_server;
+
+enum {
+  TOTEM_SCHED_FIFO = 0,          /* wave memory goes to requests in arrival order              */
+  TOTEM_SCHED_SHORTEST = 1       /* ... to the request with the least remaining work first     */
+};
+
+typedef struct TotemServerOptions {
+  int struct_size;               /* sizeof(TotemServerOptions)                                 */
+  int device;                    /* CUDA device; -1 = the one with the most free memory        */
+  unsigned long long hbm_budget; /* device bytes for all requests; 0 = 90 % of free memory     */
+  unsigned long long wave_bytes; /* of which for probe waves in flight (psi and detector
+                                    partial sums); 0 = min(8 GiB, hbm_budget / 4)               */
+  unsigned long long chunk_bytes;/* wave bytes one request may claim per tick; 0 = wave_bytes/4 */
+  int ticks_ahead;               /* slice steps queued ahead of the GPU; 0 = 4                 */
+  int policy;                    /* TOTEM_SCHED_*                                              */
+} TotemServerOptions;
+
+enum {
+  TOTEM_REQ_QUEUED = 0,          /* waiting for memory                                         */
+  TOTEM_REQ_PREPARING = 1,       /* upload and transmission build                              */
+  TOTEM_REQ_RUNNING = 2,         /* in the slice loop                                          */
+  TOTEM_REQ_DONE = 3,            /* results are in the caller's buffers                        */
+  TOTEM_REQ_FAILED = 4           /* see TotemRequestInfo.status and totem_server_info's message */
+};
+
+typedef struct TotemRequestInfo {
+  int state;                     /* TOTEM_REQ_*                                                */
+  int status;                    /* TOTEM_OK, or the error of a failed request                 */
+  double queued_ms;              /* submit -> admission                                        */
+  double prepare_ms;             /* admission -> transmission ready                            */
+  double run_ms;                 /* transmission ready -> results in the caller's buffers      */
+  double latency_ms;             /* submit -> results in the caller's buffers                  */
+  long long probe_slices;        /* w_num * depth * slices                                     */
+} TotemRequestInfo;
+
+TOTEM_API int totem_server_create(const TotemServerOptions *opt, totem_server **out);
+/* Validates the request (same checks and codes as totem_stem_run) and queues it. */
+TOTEM_API int totem_server_submit(totem_server *s, const TotemStemArgs *args, TotemStemOut *out,
+                                  unsigned long long *ticket);
+/* Blocks until the request is done or failed (returns its status) or timeout_ms passes
+ * (TOTEM_ERR_TIMEOUT; timeout_ms < 0 waits without limit). */
+TOTEM_API int totem_server_wait(totem_server *s, unsigned long long ticket, int timeout_ms);
+TOTEM_API int totem_server_info(totem_server *s, unsigned long long ticket, TotemRequestInfo *info);
+/* Finishes every queued request, then releases the device state. */
+TOTEM_API int totem_server_destroy(totem_server *s);
+
+/* The scheduler's admission policy run without a device, for tests and capacity planning:
+ * request i (window n[i], items[i] = w_num * depth probes, slices[i]) becomes ready at tick
+ * arrive[i]; a probe takes n*n*8 bytes of wave memory.  Outputs the tick of each request's first
+ * slice and of its last slice, and the largest wave memory in flight at any tick. */
+TOTEM_API int totem_plan_simulate(int count, const int *n, const long long *items, const int *slices,
+                                  const int *arrive, unsigned long long wave_bytes,
+                                  unsigned long long chunk_bytes, int policy, int *first_tick, int *done_tick,
+                                  unsigned long long *max_inflight);
 
 #ifdef __cplusplus
 } /* extern "C" */

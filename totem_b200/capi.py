@@ -17,7 +17,9 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "totem_b200.h")
 SHIM_LIBS = {("p", False): "libwaveCudaPeng.so", ("l", False): "libwaveCudaLobato.so",
              ("p", True): "libwaveCudaPengP.so", ("l", True): "libwaveCudaLobatoP.so"}
 
-OK, ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_CUFFT, ERR_OOM, ERR_NO_DEVICE, ERR_STATE = range(8)
+OK, ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_CUFFT, ERR_OOM, ERR_NO_DEVICE, ERR_STATE, ERR_TIMEOUT = range(9)
+SCHED_FIFO, SCHED_SHORTEST = 0, 1
+REQ_QUEUED, REQ_PREPARING, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
 PARAM_PENG, PARAM_LOBATO = 0, 1
 PATH_FUSED, PATH_PLAIN = 0, 1
 
@@ -59,6 +61,17 @@ class TotemTiming(C.Structure):
                 ("probe_slices", C.c_longlong), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong)]
 
 
+class TotemServerOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_int), ("device", C.c_int), ("hbm_budget", C.c_ulonglong),
+                ("wave_bytes", C.c_ulonglong), ("chunk_bytes", C.c_ulonglong), ("ticks_ahead", C.c_int),
+                ("policy", C.c_int)]
+
+
+class TotemRequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("queued_ms", C.c_double), ("prepare_ms", C.c_double),
+                ("run_ms", C.c_double), ("latency_ms", C.c_double), ("probe_slices", C.c_longlong)]
+
+
 class TotemError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"totem_b200 error {code}: {msg}")
@@ -97,9 +110,19 @@ def load() -> C.CDLL:
     lib.totem_transmission_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemStemOut)]
     lib.totem_stem_slices_noalloc.argtypes = ([vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp] + [C.c_int] * 9
                                               + [vp, vp])
+    ull, ullp = C.c_ulonglong, C.POINTER(C.c_ulonglong)
+    lib.totem_server_create.argtypes = [C.POINTER(TotemServerOptions), C.POINTER(vp)]
+    lib.totem_server_submit.argtypes = [vp, C.POINTER(TotemStemArgs), C.POINTER(TotemStemOut), ullp]
+    lib.totem_server_wait.argtypes = [vp, ull, C.c_int]
+    lib.totem_server_info.argtypes = [vp, ull, C.POINTER(TotemRequestInfo)]
+    lib.totem_server_destroy.argtypes = [vp]
+    lib.totem_plan_simulate.argtypes = [C.c_int, _ip, C.POINTER(C.c_longlong), _ip, _ip, ull, ull, C.c_int, _ip, _ip,
+                                        ullp]
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
                  "totem_session_download", "totem_session_timing", "totem_session_transmission",
-                 "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc"):
+                 "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_server_create",
+                 "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
+                 "totem_plan_simulate"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -259,6 +282,76 @@ def stem_slices_noalloc(transmission: int, p_height: int, p_width: int, slices: 
     check(lib.totem_stem_slices_noalloc(transmission, p_height, p_width, slices, probe, w_num, propagator, masks,
                                         aper_num, n, step, begin_row, begin_col, width_red, depth, item0, items,
                                         result, stream))
+
+
+class Server:
+    """The serving scheduler (``totem_server_*``): submit requests, wait for them, read latencies.
+
+    Every submitted request keeps its marshalled inputs and its output arrays referenced here
+    until it is waited for, as the C API requires.
+    """
+
+    def __init__(self, device: int = -1, hbm_budget: int = 0, wave_bytes: int = 0, chunk_bytes: int = 0,
+                 ticks_ahead: int = 0, policy: int = SCHED_SHORTEST):
+        self.lib = load()
+        o = TotemServerOptions(C.sizeof(TotemServerOptions), device, hbm_budget, wave_bytes, chunk_bytes,
+                               ticks_ahead, policy)
+        h = C.c_void_p()
+        check(self.lib.totem_server_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self._live = {}
+
+    def submit(self, req) -> int:
+        m = Marshalled(req, True)
+        res = np.zeros(req.aper_num * req.depth)
+        mid = np.zeros(req.aper_num * req.depth * len(req.mid_layer))
+        out = TotemStemOut(_ptr(res), _ptr(mid), None, None)
+        t = C.c_ulonglong()
+        check(self.lib.totem_server_submit(self.h, C.byref(m.args), C.byref(out), C.byref(t)))
+        self._live[t.value] = (m, out, res, mid)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """Results (detector sums, mid-layer sums) of a finished request; raises on failure."""
+        check(self.lib.totem_server_wait(self.h, ticket, timeout_ms))
+        _, _, res, mid = self._live.pop(ticket)
+        return res, mid
+
+    def info(self, ticket: int) -> TotemRequestInfo:
+        i = TotemRequestInfo()
+        check(self.lib.totem_server_info(self.h, ticket, C.byref(i)))
+        return i
+
+    def close(self):
+        if self.h:
+            self.lib.totem_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def plan_simulate(n, items, slices, arrive, wave_bytes: int, chunk_bytes: int = 0, policy: int = SCHED_SHORTEST):
+    """``totem_plan_simulate``: the scheduler's admission policy without a device.
+
+    Returns (first_tick, done_tick, max_inflight_bytes)."""
+    lib = load()
+    cnt = len(n)
+    n_ = np.ascontiguousarray(n, dtype=np.int32)
+    it_ = np.ascontiguousarray(items, dtype=np.int64)
+    sl_ = np.ascontiguousarray(slices, dtype=np.int32)
+    ar_ = np.ascontiguousarray(arrive, dtype=np.int32)
+    first = np.zeros(cnt, dtype=np.int32)
+    done = np.zeros(cnt, dtype=np.int32)
+    mx = C.c_ulonglong()
+    check(lib.totem_plan_simulate(cnt, n_.ctypes.data_as(_ip), it_.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                  sl_.ctypes.data_as(_ip), ar_.ctypes.data_as(_ip), wave_bytes, chunk_bytes, policy,
+                                  first.ctypes.data_as(_ip), done.ctypes.data_as(_ip), C.byref(mx)))
+    return first, done, mx.value
 
 
 def stem_run(req, path: int = PATH_FUSED, batch: int = 0):

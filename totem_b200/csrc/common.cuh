@@ -120,6 +120,32 @@ int col_blocks(int n, int variant = 0);
 Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st);
 // flags: 1 = mid-slice detectors, 2 = exit detectors, 4 = final pass (no inverse transform)
 Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st);
+// Continuous batching: one launch advances groups of items of several requests, each group at
+// its own slice (slice = tick - start_tick).  Items of a launch are numbered group by group;
+// item_begin[g] is the first launch item of group g (item_begin[ngroups] = items of the launch).
+struct GroupDesc {
+  float2* psi;                  // [items][N][N]
+  const float2* t_stack;        // [slices][p_h][p_w]
+  const float2* probe;          // [w_num][N][N]
+  const float2* prop;           // [N][N]
+  const float* mask_mid;        // [A][N][N]
+  const float* mask_exit;       // [A][N][N]
+  double* part;                 // [events][items][A][col_blocks(N)]
+  const int* event_of_slice;    // [slices + 1]: 1-based slice -> mid-layer event or -1
+  ScanGeom geo;
+  int p_h;
+  int item0;                    // first request item of the group (item = w * depth + pos)
+  int items;
+  int start_tick;
+  int slices;
+  int aper_num;
+  int exit_event;
+};
+Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                         const float2* tw, cudaStream_t st);
+Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                         const float2* tw, cudaStream_t st);
+
 // Sum the per-column-block partials in a fixed order: acc[(w*A + a)*depth + pos].
 Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth,
                          double* acc, cudaStream_t st);

@@ -20,88 +20,24 @@
 #include <string>
 #include <vector>
 
-#include "common.cuh"
+#include "session.h"
 
 using totem::Status;
+using totem::DevBuf;
+using totem::RowsHost;
+using totem::PlanKey;
+using totem::twiddles;
+using totem::upload;
+using totem::g_h2d_bytes;
 
 namespace {
 
 thread_local std::string g_last_error;
-thread_local long long g_h2d_bytes = 0;  // bytes copied host -> device by the current upload
 
 int fail(const Status& s) {
   g_last_error = s.msg;
   return s.code;
 }
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t cap = 0;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  template <class T>
-  T* as() const { return static_cast<T*>(p); }
-  Status ensure(size_t bytes) {
-    if (bytes == 0) bytes = 256;
-    if (bytes <= cap) return Status::Ok();
-    if (p) {
-      cudaFree(p);
-      p = nullptr;
-      cap = 0;
-    }
-    TOTEM_CUDA(cudaMalloc(&p, bytes));
-    cap = bytes;
-    return Status::Ok();
-  }
-};
-
-template <class T>
-Status upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
-  TOTEM_TRY(b.ensure(v.size() * sizeof(T)));
-  if (!v.empty()) TOTEM_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-  g_h2d_bytes += (long long)(v.size() * sizeof(T));
-  return Status::Ok();
-}
-
-// Stage twiddle tables of the shared-memory FFT (a one-entry placeholder for sizes it does not
-// handle; those sizes go through cuFFT).
-std::vector<float2> twiddles(int n) {
-  std::vector<float2> t = totem::stage_twiddles(n);
-  if (t.empty()) t.assign(1, make_float2(1.f, 0.f));
-  return t;
-}
-
-// Atom rows of one kind, split into FP64 positions and FP32 coefficients.
-struct RowsHost {
-  std::vector<double> pos;
-  std::vector<float> coef;
-  std::vector<float> absorp;
-  std::vector<int> beg;
-  int ncoef = 0;
-  int count = 0;
-};
-
-struct RowsDev {
-  DevBuf pos, coef, absorp, beg;
-  totem::AtomRowsDev view(bool present, bool has_absorp, int ncoef) const {
-    totem::AtomRowsDev d;
-    if (!present) return d;
-    d.pos = pos.as<double>();
-    d.coef = coef.as<float>();
-    d.absorp = has_absorp ? absorp.as<float>() : nullptr;
-    d.beg = beg.as<int>();
-    d.ncoef = ncoef;
-    return d;
-  }
-  Status put(const RowsHost& h, cudaStream_t st) {
-    TOTEM_TRY(upload(pos, h.pos, st));
-    TOTEM_TRY(upload(coef, h.coef, st));
-    TOTEM_TRY(upload(absorp, h.absorp, st));
-    TOTEM_TRY(upload(beg, h.beg, st));
-    return Status::Ok();
-  }
-};
 
 // Per-slice counts -> prefix offsets; validates that the counts are whole, non-negative numbers.
 Status offsets(const double* counts, int slices, std::vector<int>& beg, int& total, const char* what) {
@@ -138,111 +74,24 @@ RowsHost split_rows(const double* rows, int count, int ncol, const double* absor
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-struct PlanKey {
-  int h, w, batch;
-  bool operator<(const PlanKey& o) const {
-    return h != o.h ? h < o.h : (w != o.w ? w < o.w : batch < o.batch);
-  }
-};
 
 }  // namespace
 
 void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
 
-struct totem_session {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  std::mutex mu;
+thread_local long long totem::g_h2d_bytes = 0;
 
-  // request metadata
-  bool uploaded = false;
-  bool stem_ready = false;  // STEM inputs present (the transmission-only MEX passes none)
-  int param = 0, h = 0, w = 0, depth = 0, p_h = 0, p_w = 0, slices = 0, step = 0, begin_row = 0, begin_col = 0,
-      width_red = 0, w_num = 0, aper_num = 0;
-  double sigma = 0, parameter = 0;
-  std::vector<int> mid_layer;
-  std::vector<double> gfsf;
-  bool separable = false, aper_true_ones = true, has_abs_n = false, has_abs_i = false;
-  int n_rows = 0, n_rows_i = 0, n_corr = 0, n_corr_i = 0, cim_len = 0, ncoef_n = 0, ncoef_i = 0;
-
-  // device inputs
-  DevBuf probe, prop, mask_mid, mask_exit, tw_n, tw_pw, tw_ph, gfsf_d;
-  RowsDev rows_n, rows_i, rows_cn, rows_ci;
-  DevBuf kx_axis, ky_axis, kx, ky, s2, aper_true, cim;
-  // work buffers and results
-  DevBuf T, psi, part, acc, out_result, out_mid;
-  bool t_valid = false;
-  bool has_result = false;
-  int last_what = 0;
-  std::map<PlanKey, cufftHandle> plans;
-
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-  TotemTiming timing{};
-  long long h2d_bytes = 0, d2h_bytes = 0;
-  // per-launch profiling of the fused passes (TotemRunOptions.profile)
-  bool profiling = false;
-  std::vector<cudaEvent_t> pev;
-  std::vector<int> pkind;  // 0 = row pass, 1 = column pass
-  size_t pused = 0;
-
-  ~totem_session() {
-    for (auto& kv : plans) cufftDestroy(kv.second);
-    for (auto& e : ev)
-      if (e) cudaEventDestroy(e);
-    for (auto& e : pev) cudaEventDestroy(e);
-    if (own_stream && stream) cudaStreamDestroy(stream);
-  }
-
-  Status prof_begin() {
-    if (!profiling) return Status::Ok();
-    while (pev.size() < pused + 2) {
-      cudaEvent_t e;
-      TOTEM_CUDA(cudaEventCreate(&e));
-      pev.push_back(e);
-    }
-    TOTEM_CUDA(cudaEventRecord(pev[pused], stream));
-    return Status::Ok();
-  }
-  Status prof_end(int kind) {
-    if (!profiling) return Status::Ok();
-    TOTEM_CUDA(cudaEventRecord(pev[pused + 1], stream));
-    pkind.push_back(kind);
-    pused += 2;
-    return Status::Ok();
-  }
-
-  Status plan(int ph, int pw, int batch, cufftHandle* out) {
-    PlanKey k{ph, pw, batch};
-    auto it = plans.find(k);
-    if (it != plans.end()) {
-      *out = it->second;
-      return Status::Ok();
-    }
-    cufftHandle p;
-    int n[2] = {ph, pw};
-    TOTEM_CUFFT(cufftPlanMany(&p, 2, n, nullptr, 1, ph * pw, nullptr, 1, ph * pw, CUFFT_C2C, batch));
-    TOTEM_CUFFT(cufftSetStream(p, stream));
-    plans[k] = p;
-    *out = p;
-    return Status::Ok();
-  }
-
-  Status upload_args(const TotemStemArgs* a, bool stem);
-  Status build_transmission(int path, int* launches);
-  Status slice_loop(int path, int batch, int col_variant, int* launches, int* batch_used);
-  Status run(int what, const TotemRunOptions* opt);
-  Status collect_timing();
-  Status download(TotemStemOut* out);
-  bool timing_pending = false;
-};
+std::vector<float2> totem::twiddles(int n) {
+  std::vector<float2> t = totem::stage_twiddles(n);
+  if (t.empty()) t.assign(1, make_float2(1.f, 0.f));
+  return t;
+}
 
 // ---------------------------------------------------------------------------------------------
 // Upload
 // ---------------------------------------------------------------------------------------------
-Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
+Status totem_session::validate(const TotemStemArgs* a, bool stem) {
   if (a == nullptr) return Status::Err(TOTEM_ERR_INVALID_ARG, "args is NULL");
-  g_h2d_bytes = 0;
   if (a->struct_size != (int)sizeof(TotemStemArgs))
     return Status::Err(TOTEM_ERR_INVALID_ARG, "TotemStemArgs.struct_size does not match this library");
   if (a->param != TOTEM_PARAM_PENG && a->param != TOTEM_PARAM_LOBATO)
@@ -256,7 +105,6 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
   // HRTEMsimulation sets probe = [] at ToTEM_submit_v1.m:1259); STEM fields are checked only
   // when a STEM request is present.
   const bool want_stem = stem && a->depth > 0;
-  stem_ready = false;
   if (want_stem) {
     if (a->height <= 0 || a->width <= 0 || a->w_num <= 0 || a->aper_num < 0)
       return Status::Err(TOTEM_ERR_INVALID_ARG, "negative or zero window size");
@@ -277,7 +125,20 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
   }
   if (!a->kx || !a->ky || !a->s_2 || !a->aper_true)
     return Status::Err(TOTEM_ERR_INVALID_ARG, "kx, ky, s_2 and aper_true are required");
+  std::vector<int> beg;
+  int count = 0;
+  TOTEM_TRY(offsets(a->atom_slice, a->slices, beg, count, "atom_slice"));
+  if (count > 0 && !a->proj_coff_mat) return Status::Err(TOTEM_ERR_INVALID_ARG, "proj_coff_mat is NULL");
+  TOTEM_TRY(offsets(a->atom_slice_i, a->slices, beg, count, "atom_slice_i"));
+  if (count > 0 && !a->proj_coff_mat_i) return Status::Err(TOTEM_ERR_INVALID_ARG, "proj_coff_mat_i is NULL");
+  return Status::Ok();
+}
 
+Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
+  g_h2d_bytes = 0;
+  stem_ready = false;
+  TOTEM_TRY(validate(a, stem));
+  const bool want_stem = stem && a->depth > 0;
   param = a->param;
   p_h = a->p_height; p_w = a->p_width; slices = a->slices;
   sigma = a->sigma; parameter = a->parameter;
@@ -447,20 +308,9 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int* laun
     has_result = true;
     return Status::Ok();
   }
-  // detection events: every distinct valid mid-layer slice (first occurrence wins, as
-  // find(midslice==k, 1) in cuda_STEM_CPU_Mcore_lobato_peng.m:66-67) plus the exit wave.
-  std::vector<int> event_of_slice(slices + 1, -1);
-  std::vector<int> layer_event(L, -1);
-  int n_events = 0;
-  for (int l = 0; l < L; ++l) {
-    const int k = mid_layer[l];
-    if (k < 1 || k > slices) continue;
-    if (event_of_slice[k] < 0) {
-      event_of_slice[k] = n_events++;
-      layer_event[l] = event_of_slice[k];
-    }
-  }
-  const int exit_event = n_events++;
+  const totem::DetectionEvents de = detection_events();
+  const std::vector<int>& event_of_slice = de.event_of_slice;
+  const int n_events = de.n_events, exit_event = de.exit_event;
 
   const bool fused = (path == TOTEM_PATH_FUSED) && h == w && is_pow2(h) && h >= 64 && h <= 2048 && slices > 0;
   const size_t vol = (size_t)h * w;
@@ -556,17 +406,41 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int* laun
       ++*launches;
     }
   }
-  TOTEM_TRY(totem::launch_combine(acc.as<double>() + (size_t)exit_event * w_num * ad, gfsf_d.as<double>(), w_num, ad,
-                                  out_result.as<double>(), stream));
+  TOTEM_TRY(combine_results(de, launches));
+  has_result = true;
+  return Status::Ok();
+}
+
+totem::DetectionEvents totem_session::detection_events() const {
+  totem::DetectionEvents de;
+  const int L = (int)mid_layer.size();
+  de.event_of_slice.assign(slices + 1, -1);
+  de.layer_event.assign(L, -1);
+  for (int l = 0; l < L; ++l) {
+    const int k = mid_layer[l];
+    if (k < 1 || k > slices) continue;
+    if (de.event_of_slice[k] < 0) {
+      de.event_of_slice[k] = de.n_events++;
+      de.layer_event[l] = de.event_of_slice[k];
+    }
+  }
+  de.exit_event = de.n_events++;
+  return de;
+}
+
+Status totem_session::combine_results(const totem::DetectionEvents& de, int* launches) {
+  const long ad = (long)aper_num * depth;
+  const int L = (int)mid_layer.size();
+  TOTEM_TRY(totem::launch_combine(acc.as<double>() + (size_t)de.exit_event * w_num * ad, gfsf_d.as<double>(), w_num,
+                                  ad, out_result.as<double>(), stream));
   ++*launches;
   if (L > 0) TOTEM_CUDA(cudaMemsetAsync(out_mid.p, 0, (size_t)ad * L * sizeof(double), stream));
   for (int l = 0; l < L; ++l) {
-    if (layer_event[l] < 0) continue;
-    TOTEM_TRY(totem::launch_combine(acc.as<double>() + (size_t)layer_event[l] * w_num * ad, gfsf_d.as<double>(),
+    if (de.layer_event[l] < 0) continue;
+    TOTEM_TRY(totem::launch_combine(acc.as<double>() + (size_t)de.layer_event[l] * w_num * ad, gfsf_d.as<double>(),
                                     w_num, ad, out_mid.as<double>() + (size_t)l * ad, stream));
     ++*launches;
   }
-  has_result = true;
   return Status::Ok();
 }
 
@@ -661,9 +535,7 @@ Status totem_session::download(TotemStemOut* out) {
 // ---------------------------------------------------------------------------------------------
 // Device choice and the cached default sessions used by the one-shot entry points
 // ---------------------------------------------------------------------------------------------
-namespace {
-
-Status pick_device(int* dev) {
+Status totem::pick_device(int* dev) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) return Status::Err(TOTEM_ERR_NO_DEVICE, "no CUDA device visible");
@@ -684,7 +556,7 @@ Status pick_device(int* dev) {
   return Status::Ok();
 }
 
-Status create_session(int device, void* stream, totem_session** out) {
+Status totem::create_session(int device, void* stream, totem_session** out) {
   TOTEM_TRY(pick_device(&device));
   TOTEM_CUDA(cudaSetDevice(device));
   std::unique_ptr<totem_session> s(new totem_session());
@@ -698,6 +570,11 @@ Status create_session(int device, void* stream, totem_session** out) {
   *out = s.release();
   return Status::Ok();
 }
+
+namespace {
+
+using totem::create_session;
+using totem::pick_device;
 
 std::mutex g_default_mu;
 std::map<int, totem_session*> g_default;  // device -> session kept for the one-shot calls
@@ -752,6 +629,7 @@ const char* totem_status_string(int status) {
     case TOTEM_ERR_OOM: return "out of memory";
     case TOTEM_ERR_NO_DEVICE: return "no CUDA device";
     case TOTEM_ERR_STATE: return "invalid call sequence";
+    case TOTEM_ERR_TIMEOUT: return "timed out";
   }
   return "unknown status";
 }

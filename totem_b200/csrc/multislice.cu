@@ -24,23 +24,22 @@ namespace totem {
 
 namespace {
 
+// One CTA's share of a row pass: rows row0 .. row0+G-1 of one probe's wave.
+//   psi_item  the probe's wave [N][N];  t_origin  T at the window origin (row stride p_w);
+//   probe_item  the probe [N][N] (FIRST only: the first pass starts from the probe).
 template <int N, bool FIRST>
-__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) k_row_pass(SliceLoopArgs a, const float2* __restrict__ tslice,
-                                                                         float scale) {
-  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T, G = RowCfg<N>::G;
+__device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const float2* __restrict__ t_origin, long p_w,
+                                         const float2* __restrict__ probe_item, int row0, float scale,
+                                         const float2* __restrict__ tw) {
+  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
   const int g = threadIdx.x / T, j = threadIdx.x - g * T;
-  const long grow = (long)blockIdx.x * G + g;
-  const int item = (int)(grow / N), row = (int)(grow % N);
-  load_twiddles<N>(s_tw, a.tw);
-  const int gi = a.item0 + item;
-  const int w = gi / a.geo.depth, pos = gi - w * a.geo.depth;
-  const int x0 = a.geo.begin_row + (pos / a.geo.width_red) * a.geo.step + row;
-  const int y0 = a.geo.begin_col + (pos % a.geo.width_red) * a.geo.step;
-  const float2* __restrict__ trow = tslice + (long)x0 * a.geo.p_width + y0;
-  float2* prow = a.psi + ((long)item * N + row) * N;
+  const int row = row0 + g;
+  load_twiddles<N>(s_tw, tw);
+  const float2* __restrict__ trow = t_origin + (long)row * p_w;
+  float2* prow = psi_item + (long)row * N;
   const RowLayout<N> L;
   const auto sync = group_sync<N>(g);
   // The transmission window row is copied asynchronously into this row's exchange region as soon
@@ -55,7 +54,7 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) 
   float2 v[P];
   if (FIRST) {
     prefetch_t();
-    const float2* src = a.probe + ((long)w * N + row) * N;
+    const float2* src = probe_item + (long)row * N;
 #pragma unroll
     for (int m = 0; m < P; ++m) v[m] = __ldg(src + j + m * T);
   } else {
@@ -71,6 +70,20 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) 
   fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
   for (int m = 0; m < P; ++m) prow[j + m * T] = v[m];
+}
+
+template <int N, bool FIRST>
+__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
+    k_row_pass(SliceLoopArgs a, const float2* __restrict__ tslice, float scale) {
+  constexpr int G = RowCfg<N>::G;
+  const long grow0 = (long)blockIdx.x * G;  // G divides N: the CTA's rows belong to one item
+  const int item = (int)(grow0 / N), row0 = (int)(grow0 % N);
+  const int gi = a.item0 + item;
+  const int w = gi / a.geo.depth, pos = gi - w * a.geo.depth;
+  const int x0 = a.geo.begin_row + (pos / a.geo.width_red) * a.geo.step;
+  const int y0 = a.geo.begin_col + (pos % a.geo.width_red) * a.geo.step;
+  row_tile<N, FIRST>(a.psi + (long)item * N * N, tslice + (long)x0 * a.geo.p_width + y0, a.geo.p_width,
+                     a.probe + (long)w * N * N, row0, scale, a.tw);
 }
 
 // Deterministic block sum of one double per thread; result valid in thread 0.
@@ -104,24 +117,32 @@ __device__ __forceinline__ void detect(const float (&inten)[Fft<N>::P], const fl
   }
 }
 
-// Variants (measured on the SrTiO3 512^2 workload, per 4096-probe launch): the propagator read
-// straight from global memory (L2-resident) at a 128-register cap, 4.3 ms (the default); the
-// propagator column prefetched into shared memory while the forward transform finishes, 4.6 ms;
-// the direct read at an 80-register cap (6 CTAs per SM), 5.8 ms.
-template <int N, bool PREFETCH, int CTAS128, int GW>
-__global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
-    k_col_pass(SliceLoopArgs a, int flags) {
-  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N, CTAS128, GW>::G;
+// Inputs of the column pass shared by every item of a launch (or of a group).
+struct ColInputs {
+  const float2* prop;
+  const float* mask_mid;
+  const float* mask_exit;
+  int aper_num;
+  double* part_mid;   // [items][aper_num][nblk] when flags & 1
+  double* part_exit;  // [items][aper_num][nblk] when flags & 2
+};
+
+// One CTA's share of a column pass: columns cb*G .. cb*G+G-1 of one probe's wave.  ``item`` is
+// the item's index in the partial-sum arrays.  flags: 1 mid detectors, 2 exit detectors,
+// 4 final pass (no inverse transform).
+template <int N, bool PREFETCH, int G>
+__device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const ColInputs& in, int item, int cb, int flags,
+                                         const float2* __restrict__ tw) {
+  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
   __shared__ double red[32];
   constexpr int nblk = N / G;
   const int j = threadIdx.x / G, g = threadIdx.x - j * G;
-  const int item = blockIdx.x / nblk, cb = blockIdx.x - item * nblk;
   const int c = cb * G + g;
-  load_twiddles<N>(s_tw, a.tw);
-  float2* base = a.psi + (long)item * N * N + c;
+  load_twiddles<N>(s_tw, tw);
+  float2* base = psi_item + c;
   float2 v[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) v[m] = base[(long)(j + m * T) * N];
@@ -133,11 +154,11 @@ __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128,
   if constexpr (!PREFETCH) {
     fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
-    for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(a.prop + (long)(j + m * T) * N + c));
+    for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(in.prop + (long)(j + m * T) * N + c));
   } else {
     auto prefetch_h = [&]() {
 #pragma unroll
-      for (int m = 0; m < P; ++m) cp_async8(&s_x[L.pos(g, j, m)], a.prop + (long)(j + m * T) * N + c);
+      for (int m = 0; m < P; ++m) cp_async8(&s_x[L.pos(g, j, m)], in.prop + (long)(j + m * T) * N + c);
       cp_async_commit();
     };
     fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync, prefetch_h);
@@ -150,13 +171,92 @@ __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128,
     float inten[P];
 #pragma unroll
     for (int m = 0; m < P; ++m) inten[m] = fmaf(v[m].x, v[m].x, v[m].y * v[m].y);
-    if (flags & 1) detect<N>(inten, a.mask_mid, a.aper_num, j, c, a.part_mid, item, cb, nblk, red);
-    if (flags & 2) detect<N>(inten, a.mask_exit, a.aper_num, j, c, a.part_exit, item, cb, nblk, red);
+    if (flags & 1) detect<N>(inten, in.mask_mid, in.aper_num, j, c, in.part_mid, item, cb, nblk, red);
+    if (flags & 2) detect<N>(inten, in.mask_exit, in.aper_num, j, c, in.part_exit, item, cb, nblk, red);
   }
   if (flags & 4) return;
   fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
   for (int m = 0; m < P; ++m) base[(long)(j + m * T) * N] = v[m];
+}
+
+// Column-pass variants, per 2048-probe launch on the SrTiO3 512^2 workload (microseconds per
+// probe): 16-column tiles with the propagator read from global memory (L2-resident) at a
+// 128-register cap, 0.98 (the default); 8-column tiles 1.11; 32-column tiles 1.32; 16-column
+// tiles at an 80-register cap 1.10.  With 8-column tiles, prefetching the propagator into shared
+// memory (4.6 ms against 4.3 ms per 4096 probes) and an 80-register cap (5.8 ms) were slower.
+template <int N, bool PREFETCH, int CTAS128, int GW>
+__global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
+    k_col_pass(SliceLoopArgs a, int flags) {
+  constexpr int G = ColCfg<N, CTAS128, GW>::G;
+  constexpr int nblk = N / G;
+  const int item = blockIdx.x / nblk, cb = blockIdx.x - item * nblk;
+  const ColInputs in{a.prop, a.mask_mid, a.mask_exit, a.aper_num, a.part_mid, a.part_exit};
+  col_tile<N, PREFETCH, G>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw);
+}
+
+// Group of launch item ``li``: the last g with item_begin[g] <= li.
+__device__ __forceinline__ int find_group(const int* __restrict__ item_begin, int ngroups, int li) {
+  int lo = 0, hi = ngroups - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(item_begin + mid) <= li) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Row pass of a continuous batch: the same tile as k_row_pass, with the probe, transmission slice
+// and window of each item taken from its group.
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
+    k_row_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
+                 const float2* __restrict__ tw) {
+  constexpr int G = RowCfg<N>::G, per_item = N / G;
+  const int li = blockIdx.x / per_item;
+  const int row0 = (blockIdx.x - li * per_item) * G;
+  const int gidx = find_group(item_begin, ngroups, li);
+  const GroupDesc& d = groups[gidx];
+  const int item = li - __ldg(item_begin + gidx);
+  const int slice = tick - d.start_tick;
+  const int gi = d.item0 + item;
+  const int w = gi / d.geo.depth, pos = gi - w * d.geo.depth;
+  const int x0 = d.geo.begin_row + (pos / d.geo.width_red) * d.geo.step;
+  const int y0 = d.geo.begin_col + (pos % d.geo.width_red) * d.geo.step;
+  const long p_w = d.geo.p_width;
+  const float2* t_origin = d.t_stack + (long)slice * d.p_h * p_w + (long)x0 * p_w + y0;
+  float2* psi_item = d.psi + (long)item * N * N;
+  if (slice == 0)
+    row_tile<N, true>(psi_item, t_origin, p_w, d.probe + (long)w * N * N, row0, 1.f, tw);
+  else
+    row_tile<N, false>(psi_item, t_origin, p_w, nullptr, row0, 1.f / ((float)N * (float)N), tw);
+}
+
+// Column pass of a continuous batch: detectors at the group's mid-layer slices, exit detectors
+// and no inverse transform at its last slice.
+template <int N>
+__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB)
+    k_col_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
+                 const float2* __restrict__ tw) {
+  constexpr int G = ColCfg<N>::G, nblk = N / G;
+  const int li = blockIdx.x / nblk, cb = blockIdx.x - li * nblk;
+  const int gidx = find_group(item_begin, ngroups, li);
+  const GroupDesc& d = groups[gidx];
+  const int item = li - __ldg(item_begin + gidx);
+  const int slice = tick - d.start_tick;
+  const long estride = (long)d.items * d.aper_num * nblk;
+  ColInputs in{d.prop, d.mask_mid, d.mask_exit, d.aper_num, nullptr, nullptr};
+  int flags = 0;
+  const int ev = __ldg(d.event_of_slice + slice + 1);
+  if (ev >= 0) {
+    flags |= 1;
+    in.part_mid = d.part + ev * estride;
+  }
+  if (slice == d.slices - 1) {
+    flags |= 2 | 4;
+    in.part_exit = d.part + d.exit_event * estride;
+  }
+  col_tile<N, false, G>(d.psi + (long)item * N * N, in, item, cb, flags, tw);
 }
 
 __global__ void k_det_reduce(const double* __restrict__ part, int nblk, int aper_num, int items, int item0,
@@ -293,6 +393,54 @@ Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
     case 2048: return col_pass<2048>(a, flags, st);
   }
   return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused slice loop needs a power-of-two window 64..2048");
+}
+
+template <int N>
+Status row_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
+                  cudaStream_t st) {
+  constexpr int G = RowCfg<N>::G, T = RowCfg<N>::T;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_row_groups<N>, smem));
+  k_row_groups<N><<<(unsigned)(items * (N / G)), G * T, smem, st>>>(groups, item_begin, ngroups, tick, tw);
+  return cuda_status(cudaGetLastError(), "k_row_groups");
+}
+
+template <int N>
+Status col_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
+                  cudaStream_t st) {
+  constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_col_groups<N>, smem));
+  k_col_groups<N><<<(unsigned)(items * (N / G)), G * T, smem, st>>>(groups, item_begin, ngroups, tick, tw);
+  return cuda_status(cudaGetLastError(), "k_col_groups");
+}
+
+Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                         const float2* tw, cudaStream_t st) {
+  if (items <= 0 || ngroups <= 0) return Status::Ok();
+  switch (n) {
+    case 64: return row_groups<64>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 128: return row_groups<128>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 256: return row_groups<256>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 512: return row_groups<512>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 1024: return row_groups<1024>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 2048: return row_groups<2048>(groups, item_begin, ngroups, items, tick, tw, st);
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
+}
+
+Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                         const float2* tw, cudaStream_t st) {
+  if (items <= 0 || ngroups <= 0) return Status::Ok();
+  switch (n) {
+    case 64: return col_groups<64>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 128: return col_groups<128>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 256: return col_groups<256>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 512: return col_groups<512>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 1024: return col_groups<1024>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 2048: return col_groups<2048>(groups, item_begin, ngroups, items, tick, tw, st);
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
 }
 
 Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth, double* acc,

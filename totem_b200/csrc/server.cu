@@ -1,0 +1,643 @@
+// Serving runtime: a resident scheduler with continuous batching (totem_server_* in
+// include/totem_b200.h).  No counterpart in the reference, whose entry point serves one blocking
+// request at a time (waveCuda.cpp:4-101) and allocates and frees all device state per call
+// (cuda_source_lobato.cu:1018-1562).
+//
+// Three host threads per server:
+//   prep      admission against the memory budget, then upload and transmission build of one
+//             request at a time on the request's own stream (overlapping the running slice loop);
+//   schedule  the tick loop: every tick starts the probe groups the Planner admits, advances all
+//             running groups by one slice (one k_row_groups and one k_col_groups launch per window
+//             size, on the server stream), reduces the detector sums of finished groups and
+//             combines the results of finished requests;
+//   complete  copies results into the caller's buffers and retires the request's device state.
+// Device memory comes from a dedicated stream-ordered pool, so admitting and retiring requests
+// never synchronises the device.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "planner.h"
+#include "session.h"
+
+using totem::Status;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+bool fused_window(int h, int w) { return h == w && h >= 64 && h <= 2048 && (h & (h - 1)) == 0; }
+
+struct Request {
+  unsigned long long ticket = 0;
+  TotemStemArgs args{};
+  TotemStemOut out{};
+  int state = TOTEM_REQ_QUEUED;
+  int status = TOTEM_OK;
+  std::string error;
+  Clock::time_point t_submit, t_admit, t_ready, t_done;
+  size_t reserve = 0;               // resident footprint held against the budget
+  totem_session* sess = nullptr;
+  cudaEvent_t ready = nullptr;      // transmission built (session stream)
+  cudaEvent_t handoff = nullptr;    // detector sums complete (server stream)
+  cudaEvent_t done = nullptr;       // results combined (session stream)
+  totem::DetectionEvents de;
+  long long items = 0, items_left = 0;
+  int nblk = 0;
+  size_t item_bytes = 0;
+  long long probe_slices = 0;
+};
+
+// Resident bytes of a request outside its probe waves (upper estimate, pool slack included).
+size_t resident_bytes(const TotemStemArgs& a) {
+  const size_t plane = (size_t)a.p_height * a.p_width;
+  const size_t vol = (size_t)a.height * a.width;
+  size_t b = plane * (size_t)std::max(a.slices, 1) * 8;  // transmission stack
+  b += plane * (8 + 4 + 4);                             // s2, aper_true, general kx/ky share
+  b += plane * (size_t)std::max(a.cim_len, 0) * 4;
+  long long atoms = 0;
+  for (const double* cnt : {a.atom_slice, a.atom_slice_i, a.series_n_corr, a.series_n_i_corr})
+    if (cnt)
+      for (int s = 0; s < a.slices; ++s) atoms += (long long)cnt[s];
+  b += (size_t)atoms * (16 + 26 * 4 + 40);
+  b += vol * 8 * ((size_t)a.w_num + 1);                  // probes, propagator
+  b += vol * 4 * 2 * (size_t)std::max(a.aper_num, 1);    // masks
+  const size_t ad = (size_t)std::max(a.aper_num, 0) * std::max(a.depth, 0);
+  const size_t events = (size_t)std::max(a.layer_len, 0) + 1;
+  b += ad * 8 * (events * (size_t)a.w_num + events);     // acc + outputs
+  return b + (32u << 20);
+}
+
+}  // namespace
+
+struct totem_server {
+  int device = 0;
+  TotemServerOptions opt{};
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t sst = nullptr;
+  size_t static_budget = 0, static_used = 0;
+
+  std::mutex mu;
+  std::condition_variable cv;       // any state change
+  std::deque<Request*> submitted, ready, completing;
+  std::map<unsigned long long, std::unique_ptr<Request>> reqs;
+  std::map<unsigned long long, Request*> running;
+  unsigned long long next_ticket = 1;
+  bool stopping = false, prep_exited = false, sched_exited = false;
+  Status fatal;
+
+  std::thread prep_thr, sched_thr, done_thr;
+
+  // scheduler-owned device state
+  std::map<int, std::unique_ptr<totem::DevBuf>> tw;  // stage twiddles per window size
+  int K = 4;                                         // ticks queued ahead
+  size_t slot_bytes = 0;
+  char* h_stage = nullptr;                           // pinned [K][slot_bytes]
+  char* d_stage = nullptr;                           // device [K][slot_bytes]
+  std::vector<cudaEvent_t> tick_ev;
+  size_t max_groups = 4096;
+
+  Status init();
+  void prep_loop();
+  void sched_loop();
+  void done_loop();
+  Status prepare(Request* r);
+  Status tick_once(totem::Planner& planner, int tick, bool* progressed);
+  Status complete_request(Request* r);
+  void fail_request(Request* r, const Status& s);
+  void fail_all(const Status& s);
+};
+
+Status totem_server::init() {
+  TOTEM_CUDA(cudaSetDevice(device));
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  TOTEM_CUDA(cudaMemPoolCreate(&pool, &props));
+  unsigned long long keep = ~0ull;  // keep freed memory in the pool for the next request
+  TOTEM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  TOTEM_CUDA(cudaStreamCreateWithFlags(&sst, cudaStreamNonBlocking));
+  size_t fr = 0, tot = 0;
+  TOTEM_CUDA(cudaMemGetInfo(&fr, &tot));
+  size_t budget = opt.hbm_budget ? (size_t)opt.hbm_budget : (size_t)(0.9 * (double)fr);
+  size_t wave = opt.wave_bytes ? (size_t)opt.wave_bytes : std::min<size_t>(8ull << 30, budget / 4);
+  if (wave >= budget) return Status::Err(TOTEM_ERR_INVALID_ARG, "wave_bytes must be below hbm_budget");
+  opt.hbm_budget = budget;
+  opt.wave_bytes = wave;
+  if (!opt.chunk_bytes) opt.chunk_bytes = wave / 4;
+  static_budget = budget - wave;
+  K = opt.ticks_ahead > 0 ? opt.ticks_ahead : 4;
+  slot_bytes = max_groups * (sizeof(totem::GroupDesc) + sizeof(int)) + 64 * (sizeof(int) + 256);
+  TOTEM_CUDA(cudaMallocHost(&h_stage, slot_bytes * K));
+  TOTEM_CUDA(cudaMalloc(&d_stage, slot_bytes * K));
+  tick_ev.assign(K, nullptr);
+  for (auto& e : tick_ev) TOTEM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return Status::Ok();
+}
+
+void totem_server::fail_request(Request* r, const Status& s) {
+  // caller holds ``mu``
+  r->state = TOTEM_REQ_FAILED;
+  r->status = s.code;
+  r->error = s.msg;
+  r->t_done = Clock::now();
+}
+
+void totem_server::fail_all(const Status& s) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (fatal.ok()) fatal = s;
+  for (auto& kv : reqs)
+    if (kv.second->state != TOTEM_REQ_DONE && kv.second->state != TOTEM_REQ_FAILED) fail_request(kv.second.get(), s);
+  submitted.clear();
+  ready.clear();
+  running.clear();
+  cv.notify_all();
+}
+
+// ---------------------------------------------------------------------------------------------
+// prep: admission, upload, transmission build
+// ---------------------------------------------------------------------------------------------
+Status totem_server::prepare(Request* r) {
+  TOTEM_CUDA(cudaSetDevice(device));
+  totem_session* s = nullptr;
+  TOTEM_TRY(totem::create_session(device, nullptr, &s));
+  r->sess = s;
+  s->use_pool(pool);
+  TOTEM_TRY(s->upload_args(&r->args, true));
+  int launches = 0;
+  TOTEM_TRY(s->build_transmission(TOTEM_PATH_FUSED, &launches));
+  r->de = s->detection_events();
+  TOTEM_TRY(totem::upload(s->ev_slice, r->de.event_of_slice, s->stream));
+  const size_t ad = (size_t)s->aper_num * s->depth;
+  const size_t L = s->mid_layer.size();
+  const size_t acc_n = (size_t)r->de.n_events * s->w_num * ad;
+  TOTEM_TRY(s->acc.ensure(std::max<size_t>(acc_n, 1) * sizeof(double)));
+  if (acc_n) TOTEM_CUDA(cudaMemsetAsync(s->acc.p, 0, acc_n * sizeof(double), s->stream));
+  TOTEM_TRY(s->out_result.ensure(std::max<size_t>(ad, 1) * sizeof(double)));
+  TOTEM_TRY(s->out_mid.ensure(std::max<size_t>(ad * L, 1) * sizeof(double)));
+  r->items = (s->aper_num > 0) ? (long long)s->w_num * s->depth : 0;
+  r->items_left = r->items;
+  r->nblk = totem::col_blocks(s->h);
+  r->item_bytes = (size_t)s->h * s->w * sizeof(float2) + (size_t)r->de.n_events * s->aper_num * r->nblk * sizeof(double);
+  r->probe_slices = (long long)s->w_num * s->depth * s->slices;
+  TOTEM_CUDA(cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming));
+  TOTEM_CUDA(cudaEventCreateWithFlags(&r->handoff, cudaEventDisableTiming));
+  TOTEM_CUDA(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming));
+  TOTEM_CUDA(cudaEventRecord(r->ready, s->stream));
+  return Status::Ok();
+}
+
+void totem_server::prep_loop() {
+  cudaSetDevice(device);
+  for (;;) {
+    Request* r = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return !submitted.empty() || stopping || !fatal.ok(); });
+      if (submitted.empty() || !fatal.ok()) break;
+      r = submitted.front();
+      // a request larger than the whole budget is admitted alone
+      cv.wait(lk, [&] {
+        return static_used + r->reserve <= static_budget || static_used == 0 || !fatal.ok();
+      });
+      if (!fatal.ok()) break;
+      submitted.pop_front();
+      static_used += r->reserve;
+      r->state = TOTEM_REQ_PREPARING;
+      r->t_admit = Clock::now();
+    }
+    const Status st = prepare(r);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!st.ok()) {
+      fail_request(r, st);
+      if (r->sess) {
+        cudaStreamSynchronize(r->sess->stream);
+        delete r->sess;
+        r->sess = nullptr;
+      }
+      static_used -= r->reserve;
+    } else {
+      ready.push_back(r);
+    }
+    cv.notify_all();
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  prep_exited = true;
+  cv.notify_all();
+}
+
+// ---------------------------------------------------------------------------------------------
+// schedule: the tick loop
+// ---------------------------------------------------------------------------------------------
+Status totem_server::complete_request(Request* r) {
+  totem_session* s = r->sess;
+  TOTEM_CUDA(cudaEventRecord(r->handoff, sst));
+  TOTEM_CUDA(cudaStreamWaitEvent(s->stream, r->handoff, 0));
+  int launches = 0;
+  if (r->items > 0) TOTEM_TRY(s->combine_results(r->de, &launches));
+  s->has_result = true;
+  s->last_what = 0;
+  TOTEM_CUDA(cudaEventRecord(r->done, s->stream));
+  std::lock_guard<std::mutex> lk(mu);
+  running.erase(r->ticket);
+  completing.push_back(r);
+  cv.notify_all();
+  return Status::Ok();
+}
+
+Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progressed) {
+  *progressed = false;
+  const int slot = tick % K;
+  TOTEM_CUDA(cudaEventSynchronize(tick_ev[slot]));  // tick - K has finished: its staging slot is free
+  // start the admitted groups
+  std::vector<totem::PlanGroup> started = planner.start(tick);
+  for (const totem::PlanGroup& g : started) {
+    Request* r = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      r = running.at(g.req);
+    }
+    void* psi = nullptr;
+    void* part = nullptr;
+    TOTEM_CUDA(cudaMallocFromPoolAsync(&psi, (size_t)g.items * g.n * g.n * sizeof(float2), pool, sst));
+    const size_t pb = (size_t)r->de.n_events * g.items * r->sess->aper_num * r->nblk * sizeof(double);
+    TOTEM_CUDA(cudaMallocFromPoolAsync(&part, std::max<size_t>(pb, 8), pool, sst));
+    planner.attach(g, psi, part);
+  }
+  const std::vector<totem::PlanGroup>& act = planner.active();
+  if (act.empty()) return Status::Ok();
+  *progressed = true;
+  // one row and one column launch per window size over every active group
+  std::map<int, std::vector<const totem::PlanGroup*>> by_n;
+  for (const totem::PlanGroup& g : act) by_n[g.n].push_back(&g);
+  char* h = h_stage + (size_t)slot * slot_bytes;
+  char* d = d_stage + (size_t)slot * slot_bytes;
+  size_t off = 0;
+  for (auto& kv : by_n) {
+    const int n = kv.first;
+    const std::vector<const totem::PlanGroup*>& gs = kv.second;
+    auto& twb = tw[n];
+    if (!twb) {
+      twb.reset(new totem::DevBuf());
+      TOTEM_TRY(totem::upload(*twb, totem::twiddles(n), sst));
+    }
+    const size_t ng = gs.size();
+    const size_t desc_off = off, ib_off = off + ng * sizeof(totem::GroupDesc);
+    off = ib_off + (ng + 1) * sizeof(int);
+    off = (off + 255) & ~(size_t)255;
+    if (off > slot_bytes) return Status::Err(TOTEM_ERR_STATE, "scheduler staging slot overflow");
+    auto* desc = reinterpret_cast<totem::GroupDesc*>(h + desc_off);
+    auto* ib = reinterpret_cast<int*>(h + ib_off);
+    long long items = 0;
+    for (size_t i = 0; i < ng; ++i) {
+      const totem::PlanGroup& g = *gs[i];
+      Request* r;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        r = running.at(g.req);
+      }
+      const totem_session* s = r->sess;
+      totem::GroupDesc& x = desc[i];
+      x.psi = static_cast<float2*>(g.psi);
+      x.t_stack = s->T.as<float2>();
+      x.probe = s->probe.as<float2>();
+      x.prop = s->prop.as<float2>();
+      x.mask_mid = s->mask_mid.as<float>();
+      x.mask_exit = s->mask_exit.as<float>();
+      x.part = static_cast<double*>(g.part);
+      x.event_of_slice = s->ev_slice.as<int>();
+      x.geo = totem::ScanGeom{s->begin_row, s->begin_col, s->step, s->width_red, s->depth, s->p_w};
+      x.p_h = s->p_h;
+      x.item0 = (int)g.item0;
+      x.items = g.items;
+      x.start_tick = g.start_tick;
+      x.slices = s->slices;
+      x.aper_num = s->aper_num;
+      x.exit_event = r->de.exit_event;
+      ib[i] = (int)items;
+      items += g.items;
+    }
+    ib[ng] = (int)items;
+    TOTEM_CUDA(cudaMemcpyAsync(d + desc_off, h + desc_off, off - desc_off, cudaMemcpyHostToDevice, sst));
+    const auto* dd = reinterpret_cast<const totem::GroupDesc*>(d + desc_off);
+    const auto* dib = reinterpret_cast<const int*>(d + ib_off);
+    TOTEM_TRY(totem::launch_row_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
+    TOTEM_TRY(totem::launch_col_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
+  }
+  // groups that ran their last slice: detector sums, then their wave memory goes back
+  for (const totem::PlanGroup& g : planner.finish(tick)) {
+    Request* r;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      r = running.at(g.req);
+    }
+    const totem_session* s = r->sess;
+    const long ad = (long)s->aper_num * s->depth;
+    const size_t estride = (size_t)g.items * s->aper_num * r->nblk;
+    for (int e = 0; e < r->de.n_events; ++e)
+      TOTEM_TRY(totem::launch_det_reduce(static_cast<const double*>(g.part) + e * estride, r->nblk, s->aper_num,
+                                         g.items, (int)g.item0, s->depth,
+                                         s->acc.as<double>() + (size_t)e * s->w_num * ad, sst));
+    TOTEM_CUDA(cudaFreeAsync(g.psi, sst));
+    TOTEM_CUDA(cudaFreeAsync(g.part, sst));
+    r->items_left -= g.items;
+    if (r->items_left == 0) TOTEM_TRY(complete_request(r));
+  }
+  TOTEM_CUDA(cudaEventRecord(tick_ev[slot], sst));
+  return Status::Ok();
+}
+
+void totem_server::sched_loop() {
+  cudaSetDevice(device);
+  totem::Planner planner(opt.wave_bytes, opt.chunk_bytes, opt.policy, max_groups);
+  int tick = 0;
+  for (;;) {
+    std::vector<Request*> fresh;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return !ready.empty() || !planner.idle() || (stopping && prep_exited) || !fatal.ok(); });
+      if (!fatal.ok()) break;
+      if (ready.empty() && planner.idle() && stopping && prep_exited) break;
+      while (!ready.empty()) {
+        fresh.push_back(ready.front());
+        ready.pop_front();
+      }
+      for (Request* r : fresh) {
+        r->state = TOTEM_REQ_RUNNING;
+        r->t_ready = Clock::now();
+        running[r->ticket] = r;
+      }
+    }
+    Status st;
+    for (Request* r : fresh) {
+      st = totem::cuda_status(cudaStreamWaitEvent(sst, r->ready, 0), "cudaStreamWaitEvent");
+      if (!st.ok()) break;
+      if (r->items == 0) {
+        st = complete_request(r);
+        if (!st.ok()) break;
+        continue;
+      }
+      totem::PlanRequest pr;
+      pr.id = r->ticket;
+      pr.n = r->sess->h;
+      pr.items = r->items;
+      pr.slices = r->sess->slices;
+      pr.item_bytes = r->item_bytes;
+      planner.add(pr);
+    }
+    bool progressed = false;
+    if (st.ok() && !planner.idle()) {
+      st = tick_once(planner, tick, &progressed);
+      if (progressed) ++tick;
+    }
+    if (!st.ok()) {
+      fail_all(st);
+      break;
+    }
+  }
+  cudaStreamSynchronize(sst);
+  std::lock_guard<std::mutex> lk(mu);
+  sched_exited = true;
+  cv.notify_all();
+}
+
+// ---------------------------------------------------------------------------------------------
+// complete: results to the caller, retire device state
+// ---------------------------------------------------------------------------------------------
+void totem_server::done_loop() {
+  cudaSetDevice(device);
+  for (;;) {
+    Request* r = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return !completing.empty() || (sched_exited && prep_exited); });
+      if (completing.empty()) break;
+      r = completing.front();
+      completing.pop_front();
+    }
+    Status st = totem::cuda_status(cudaEventSynchronize(r->done), "cudaEventSynchronize");
+    if (st.ok()) st = r->sess->download(&r->out);
+    delete r->sess;
+    r->sess = nullptr;
+    for (cudaEvent_t* e : {&r->ready, &r->handoff, &r->done})
+      if (*e) {
+        cudaEventDestroy(*e);
+        *e = nullptr;
+      }
+    std::lock_guard<std::mutex> lk(mu);
+    static_used -= r->reserve;
+    if (st.ok()) {
+      r->state = TOTEM_REQ_DONE;
+      r->status = TOTEM_OK;
+      r->t_done = Clock::now();
+    } else {
+      fail_request(r, st);
+    }
+    cv.notify_all();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+int server_fail(const Status& s) {
+  totem::set_last_error(s.msg);
+  return s.code;
+}
+
+void shutdown(totem_server* s) {
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+    s->cv.notify_all();
+  }
+  if (s->prep_thr.joinable()) s->prep_thr.join();
+  if (s->sched_thr.joinable()) s->sched_thr.join();
+  if (s->done_thr.joinable()) s->done_thr.join();
+  cudaSetDevice(s->device);
+  for (auto& kv : s->reqs)
+    if (kv.second->sess) {
+      cudaStreamSynchronize(kv.second->sess->stream);
+      delete kv.second->sess;
+      kv.second->sess = nullptr;
+    }
+  s->tw.clear();
+  if (s->sst) cudaStreamSynchronize(s->sst);
+  for (auto& e : s->tick_ev)
+    if (e) cudaEventDestroy(e);
+  if (s->h_stage) cudaFreeHost(s->h_stage);
+  if (s->d_stage) cudaFree(s->d_stage);
+  if (s->sst) cudaStreamDestroy(s->sst);
+  if (s->pool) {
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(s->pool);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int totem_server_create(const TotemServerOptions* opt, totem_server** out) {
+  if (!out) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "out is NULL"));
+  *out = nullptr;
+  TotemServerOptions o{};
+  o.struct_size = (int)sizeof(TotemServerOptions);
+  o.device = -1;
+  if (opt) {
+    if (opt->struct_size != (int)sizeof(TotemServerOptions))
+      return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "TotemServerOptions.struct_size does not match this library"));
+    o = *opt;
+  }
+  if (o.policy != TOTEM_SCHED_FIFO && o.policy != TOTEM_SCHED_SHORTEST)
+    return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "unknown scheduling policy"));
+  int dev = o.device;
+  Status st = totem::pick_device(&dev);
+  if (!st.ok()) return server_fail(st);
+  std::unique_ptr<totem_server> s(new totem_server());
+  s->device = dev;
+  s->opt = o;
+  st = s->init();
+  if (!st.ok()) {
+    shutdown(s.get());
+    return server_fail(st);
+  }
+  totem_server* raw = s.get();
+  raw->prep_thr = std::thread([raw] { raw->prep_loop(); });
+  raw->sched_thr = std::thread([raw] { raw->sched_loop(); });
+  raw->done_thr = std::thread([raw] { raw->done_loop(); });
+  *out = s.release();
+  return TOTEM_OK;
+}
+
+int totem_server_submit(totem_server* s, const TotemStemArgs* args, TotemStemOut* out, unsigned long long* ticket) {
+  if (!s || !ticket) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "NULL argument"));
+  Status st = totem_session::validate(args, true);
+  if (!st.ok()) return server_fail(st);
+  if (args->depth > 0 && !fused_window(args->height, args->width))
+    return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server runs square power-of-two windows of 64..2048"));
+  if (args->depth > 0 && args->slices < 1)
+    return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server needs at least one slice"));
+  std::unique_ptr<Request> r(new Request());
+  r->args = *args;
+  if (out) r->out = *out;
+  r->reserve = resident_bytes(*args);
+  r->t_submit = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->fatal.ok()) return server_fail(s->fatal);
+  if (s->stopping) return server_fail(Status::Err(TOTEM_ERR_STATE, "server is shutting down"));
+  r->ticket = s->next_ticket++;
+  *ticket = r->ticket;
+  s->submitted.push_back(r.get());
+  s->reqs[r->ticket] = std::move(r);
+  s->cv.notify_all();
+  return TOTEM_OK;
+}
+
+int totem_server_wait(totem_server* s, unsigned long long ticket, int timeout_ms) {
+  if (!s) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "server is NULL"));
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "unknown ticket"));
+  Request* r = it->second.get();
+  auto finished = [&] { return r->state == TOTEM_REQ_DONE || r->state == TOTEM_REQ_FAILED; };
+  if (timeout_ms < 0) s->cv.wait(lk, finished);
+  else if (!s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished))
+    return server_fail(Status::Err(TOTEM_ERR_TIMEOUT, "request not finished"));
+  if (r->status != TOTEM_OK) return server_fail(Status::Err(r->status, r->error));
+  return TOTEM_OK;
+}
+
+int totem_server_info(totem_server* s, unsigned long long ticket, TotemRequestInfo* info) {
+  if (!s || !info) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "NULL argument"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "unknown ticket"));
+  const Request* r = it->second.get();
+  *info = TotemRequestInfo{};
+  info->state = r->state;
+  info->status = r->status;
+  const bool done = r->state == TOTEM_REQ_DONE || r->state == TOTEM_REQ_FAILED;
+  if (r->state >= TOTEM_REQ_PREPARING && r->t_admit != Clock::time_point()) info->queued_ms = ms_between(r->t_submit, r->t_admit);
+  if (r->t_ready != Clock::time_point()) info->prepare_ms = ms_between(r->t_admit, r->t_ready);
+  if (done && r->t_ready != Clock::time_point()) info->run_ms = ms_between(r->t_ready, r->t_done);
+  if (done) info->latency_ms = ms_between(r->t_submit, r->t_done);
+  info->probe_slices = (long long)r->args.w_num * r->args.depth * r->args.slices;
+  if (r->state == TOTEM_REQ_FAILED) totem::set_last_error(r->error);
+  return TOTEM_OK;
+}
+
+int totem_server_destroy(totem_server* s) {
+  if (!s) return TOTEM_OK;
+  shutdown(s);
+  delete s;
+  return TOTEM_OK;
+}
+
+int totem_plan_simulate(int count, const int* n, const long long* items, const int* slices, const int* arrive,
+                        unsigned long long wave_bytes, unsigned long long chunk_bytes, int policy, int* first_tick,
+                        int* done_tick, unsigned long long* max_inflight) {
+  if (count < 0 || (count > 0 && (!n || !items || !slices || !arrive || !first_tick || !done_tick)) || !max_inflight)
+    return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "NULL argument"));
+  if (policy != TOTEM_SCHED_FIFO && policy != TOTEM_SCHED_SHORTEST)
+    return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "unknown scheduling policy"));
+  if (wave_bytes == 0) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "wave_bytes is 0"));
+  std::vector<int> order(count);
+  std::vector<long long> left(count);
+  for (int i = 0; i < count; ++i) {
+    if (n[i] <= 0 || items[i] < 0 || slices[i] < 1 || arrive[i] < 0)
+      return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "request sizes out of range"));
+    order[i] = i;
+    left[i] = items[i];
+    first_tick[i] = done_tick[i] = -1;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return arrive[a] < arrive[b]; });
+  totem::Planner planner(wave_bytes, chunk_bytes ? chunk_bytes : wave_bytes / 4, policy, 4096);
+  *max_inflight = 0;
+  size_t added = 0;
+  int remaining = count;
+  for (long long tick = 0; remaining > 0; ++tick) {
+    if (tick > (1ll << 30)) return server_fail(Status::Err(TOTEM_ERR_STATE, "simulation does not terminate"));
+    while (added < order.size() && arrive[order[added]] <= tick) {
+      const int i = order[added++];
+      if (items[i] == 0) {
+        first_tick[i] = done_tick[i] = (int)tick;
+        --remaining;
+        continue;
+      }
+      totem::PlanRequest r;
+      r.id = (unsigned long long)i;
+      r.n = n[i];
+      r.items = items[i];
+      r.slices = slices[i];
+      r.item_bytes = (size_t)n[i] * n[i] * sizeof(float2);
+      planner.add(r);
+    }
+    for (const totem::PlanGroup& g : planner.start((int)tick))
+      if (first_tick[g.req] < 0) first_tick[g.req] = (int)tick;
+    *max_inflight = std::max<unsigned long long>(*max_inflight, planner.inflight());
+    for (const totem::PlanGroup& g : planner.finish((int)tick)) {
+      left[g.req] -= g.items;
+      if (left[g.req] == 0) {
+        done_tick[g.req] = (int)tick;
+        --remaining;
+      }
+    }
+  }
+  return TOTEM_OK;
+}
+
+}  // extern "C"
