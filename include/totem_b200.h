@@ -219,7 +219,8 @@ typedef struct totem_server totem_server;
 
 enum {
   TOTEM_SCHED_FIFO = 0,          /* wave memory goes to requests in arrival order              */
-  TOTEM_SCHED_SHORTEST = 1       /* ... to the request with the least remaining work first     */
+  TOTEM_SCHED_SHORTEST = 1       /* ... to the request with the least remaining work first, and
+                                    preparation takes the cheapest queued request first         */
 };
 
 typedef struct TotemServerOptions {
@@ -227,7 +228,9 @@ typedef struct TotemServerOptions {
   int device;                    /* CUDA device; -1 = the one with the most free memory        */
   unsigned long long hbm_budget; /* device bytes for all requests; 0 = 90 % of free memory     */
   unsigned long long wave_bytes; /* of which for probe waves in flight (psi and detector
-                                    partial sums); 0 = min(8 GiB, hbm_budget / 4)               */
+                                    partial sums); 0 = min(1 GiB, hbm_budget / 4).  It bounds
+                                    the duration of a tick, hence the slice-loop latency of a
+                                    small request running beside large ones                   */
   unsigned long long chunk_bytes;/* wave bytes one request may claim per tick; 0 = wave_bytes/4 */
   int ticks_ahead;               /* slice steps queued ahead of the GPU; 0 = 4                 */
   int policy;                    /* TOTEM_SCHED_*                                              */

@@ -79,10 +79,27 @@ struct TxGrid {
   int cim_len = 0;
 };
 
-// V_k(g) * PARAMETER * APERTURE for all slices into out[slice][p_h][p_w] (complex64).
+// Atoms of one kind grouped by species, i.e. by identical coefficient (and absorptive) rows, so
+// that V(g) = sum_species f_species(s^2) * sum_atoms exp(-2 pi i g.r).
+struct SpeciesDev {
+  const double* pos = nullptr;     // [n][2] x, y, ordered by (slice, species, row order)
+  const float* coef = nullptr;     // [species][ncoef]
+  const float* absorp = nullptr;   // [species][10] or null
+  const int* seg_beg = nullptr;    // [slices + 1] first segment of every slice
+  const int* seg = nullptr;        // [segments][3]: species, first atom, end atom
+  int ncoef = 0;
+};
+
+// V_k(g) * PARAMETER * APERTURE for all slices into out[slice][p_h][p_w] (complex64), one
+// thread per pixel and atom row.  accumulate: add to out instead of overwriting it.
 Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const AtomRowsDev& ion,
                            const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out,
-                           cudaStream_t st);
+                           cudaStream_t st, bool accumulate = false);
+// The neutral and ionic terms of the same sum on separable grids, by species: a complex rank-K
+// update per species (no exponential per atom and pixel), then the form factor once per species
+// and pixel.  Overwrites out.
+Status launch_tx_species(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, float2* out,
+                         cudaStream_t st);
 // In-place unnormalised inverse 2-D FFT of every slice, times (-1)^(r+c) (the ifftshift of the
 // input), then T = exp(i * sigma_scaled * V).  Powers of two only; returns
 // TOTEM_ERR_UNSUPPORTED otherwise.

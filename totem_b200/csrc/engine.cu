@@ -74,6 +74,46 @@ RowsHost split_rows(const double* rows, int count, int ncol, const double* absor
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// Rows grouped by species: within every slice, atoms whose coefficient row (and absorptive row)
+// are identical share one form factor.  Species keep their order of first appearance in the
+// slice and atoms their row order within a species.
+totem::SpeciesHost group_species(const RowsHost& h, int slices) {
+  totem::SpeciesHost sp;
+  sp.ncoef = h.ncoef;
+  sp.seg_beg.assign(slices + 1, 0);
+  sp.pos.reserve(h.pos.size());
+  const bool ab = !h.absorp.empty();
+  std::map<std::vector<float>, int> ids;
+  std::vector<float> key;
+  for (int s = 0; s < slices && h.count > 0; ++s) {
+    std::vector<int> order;              // species in order of appearance in this slice
+    std::map<int, std::vector<int>> atoms;
+    for (int a = h.beg[s]; a < h.beg[s + 1]; ++a) {
+      key.assign(h.coef.begin() + (size_t)a * h.ncoef, h.coef.begin() + (size_t)(a + 1) * h.ncoef);
+      if (ab) key.insert(key.end(), h.absorp.begin() + (size_t)a * 10, h.absorp.begin() + (size_t)(a + 1) * 10);
+      auto it = ids.find(key);
+      if (it == ids.end()) {
+        it = ids.emplace(key, (int)ids.size()).first;
+        sp.coef.insert(sp.coef.end(), key.begin(), key.begin() + h.ncoef);
+        if (ab) sp.absorp.insert(sp.absorp.end(), key.begin() + h.ncoef, key.end());
+      }
+      auto& v = atoms[it->second];
+      if (v.empty()) order.push_back(it->second);
+      v.push_back(a);
+    }
+    for (int id : order) {
+      const int first = (int)(sp.pos.size() / 2);
+      for (int a : atoms[id]) {
+        sp.pos.push_back(h.pos[2 * (size_t)a]);
+        sp.pos.push_back(h.pos[2 * (size_t)a + 1]);
+      }
+      sp.seg.insert(sp.seg.end(), {id, first, (int)(sp.pos.size() / 2)});
+    }
+    sp.seg_beg[s + 1] = (int)(sp.seg.size() / 3);
+  }
+  return sp;
+}
+
 
 }  // namespace
 
@@ -171,8 +211,8 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
   has_abs_i = a->absorp_n_i != nullptr && n_rows_i > 0;
   ncoef_n = nc_n - 2;
   ncoef_i = nc_i - 2;
-  TOTEM_TRY(rows_n.put(split_rows(a->proj_coff_mat, n_rows, nc_n, has_abs_n ? a->absorp_n : nullptr, beg_n), st));
-  TOTEM_TRY(rows_i.put(split_rows(a->proj_coff_mat_i, n_rows_i, nc_i, has_abs_i ? a->absorp_n_i : nullptr, beg_i), st));
+  const RowsHost host_n = split_rows(a->proj_coff_mat, n_rows, nc_n, has_abs_n ? a->absorp_n : nullptr, beg_n);
+  const RowsHost host_i = split_rows(a->proj_coff_mat_i, n_rows_i, nc_i, has_abs_i ? a->absorp_n_i : nullptr, beg_i);
   cim_len = a->cim_len;
   n_corr = n_corr_i = 0;
   if (cim_len > 0) {
@@ -198,6 +238,14 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
         separable = false;
         break;
       }
+  // neutral / ionic rows: by species on separable grids (k_tx_species), row by row otherwise
+  if (separable) {
+    TOTEM_TRY(species_n.put(group_species(host_n, slices), st));
+    TOTEM_TRY(species_i.put(group_species(host_i, slices), st));
+  } else {
+    TOTEM_TRY(rows_n.put(host_n, st));
+    TOTEM_TRY(rows_i.put(host_i, st));
+  }
   std::vector<float> s2f(plane);
   for (size_t i = 0; i < plane; ++i) s2f[i] = (float)a->s_2[i];
   TOTEM_TRY(upload(s2, s2f, st));
@@ -273,12 +321,24 @@ Status totem_session::build_transmission(int path, int* launches) {
   g.lobato = (param == TOTEM_PARAM_LOBATO);
   g.cim = cim_len > 0 ? cim.as<float>() : nullptr;
   g.cim_len = cim_len;
-  const auto vn = rows_n.view(n_rows > 0, has_abs_n, ncoef_n);
-  const auto vi = rows_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
   const auto vcn = rows_cn.view(cim_len > 0 && n_corr > 0, false, 3);
   const auto vci = rows_ci.view(cim_len > 0 && n_corr_i > 0, false, 6);
-  TOTEM_TRY(totem::launch_tx_structure(g, vn, vi, vcn, vci, T.as<float2>(), stream));
-  ++*launches;
+  if (separable) {
+    const auto sn = species_n.view(n_rows > 0, has_abs_n, ncoef_n);
+    const auto si = species_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
+    TOTEM_TRY(totem::launch_tx_species(g, sn, si, T.as<float2>(), stream));
+    ++*launches;
+    if (vcn.beg || vci.beg) {  // Peng-extended correction rows: per-pixel maps, row by row
+      TOTEM_TRY(totem::launch_tx_structure(g, totem::AtomRowsDev{}, totem::AtomRowsDev{}, vcn, vci, T.as<float2>(),
+                                           stream, true));
+      ++*launches;
+    }
+  } else {
+    const auto vn = rows_n.view(n_rows > 0, has_abs_n, ncoef_n);
+    const auto vi = rows_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
+    TOTEM_TRY(totem::launch_tx_structure(g, vn, vi, vcn, vci, T.as<float2>(), stream));
+    ++*launches;
+  }
   const float sig = (float)(sigma / 1000.0);
   if (path == TOTEM_PATH_FUSED && totem::fused_fft_size_ok(p_h) && totem::fused_fft_size_ok(p_w)) {
     TOTEM_TRY(totem::launch_tx_fft_exp(T.as<float2>(), slices, p_h, p_w, sig, tw_pw.as<float2>(),

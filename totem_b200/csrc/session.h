@@ -90,6 +90,39 @@ struct RowsDev {
   }
 };
 
+// Atom rows of one kind grouped by species (identical coefficient and absorptive rows).
+struct SpeciesHost {
+  std::vector<double> pos;     // [n][2] ordered by (slice, species, row order)
+  std::vector<float> coef;     // [species][ncoef]
+  std::vector<float> absorp;   // [species][10] (rows with absorptive coefficients)
+  std::vector<int> seg_beg;    // [slices + 1]
+  std::vector<int> seg;        // [segments][3]: species, first atom, end atom
+  int ncoef = 0;
+};
+
+struct SpeciesRowsDev {
+  DevBuf pos, coef, absorp, seg_beg, seg;
+  SpeciesDev view(bool present, bool has_absorp, int ncoef) const {
+    SpeciesDev d;
+    if (!present) return d;
+    d.pos = pos.as<double>();
+    d.coef = coef.as<float>();
+    d.absorp = has_absorp ? absorp.as<float>() : nullptr;
+    d.seg_beg = seg_beg.as<int>();
+    d.seg = seg.as<int>();
+    d.ncoef = ncoef;
+    return d;
+  }
+  Status put(const SpeciesHost& h, cudaStream_t st) {
+    TOTEM_TRY(upload(pos, h.pos, st));
+    TOTEM_TRY(upload(coef, h.coef, st));
+    TOTEM_TRY(upload(absorp, h.absorp, st));
+    TOTEM_TRY(upload(seg_beg, h.seg_beg, st));
+    TOTEM_TRY(upload(seg, h.seg, st));
+    return Status::Ok();
+  }
+};
+
 struct PlanKey {
   int h, w, batch;
   bool operator<(const PlanKey& o) const {
@@ -129,6 +162,7 @@ struct totem_session {
   // device inputs
   totem::DevBuf probe, prop, mask_mid, mask_exit, tw_n, tw_pw, tw_ph, gfsf_d;
   totem::RowsDev rows_n, rows_i, rows_cn, rows_ci;
+  totem::SpeciesRowsDev species_n, species_i;  // the neutral / ionic rows by species (separable grids)
   totem::DevBuf kx_axis, ky_axis, kx, ky, s2, aper_true, cim;
   // work buffers and results
   totem::DevBuf T, psi, part, acc, out_result, out_mid;
@@ -165,6 +199,8 @@ struct totem_session {
       f(*b);
     for (totem::RowsDev* r : {&rows_n, &rows_i, &rows_cn, &rows_ci})
       for (totem::DevBuf* b : {&r->pos, &r->coef, &r->absorp, &r->beg}) f(*b);
+    for (totem::SpeciesRowsDev* r : {&species_n, &species_i})
+      for (totem::DevBuf* b : {&r->pos, &r->coef, &r->absorp, &r->seg_beg, &r->seg}) f(*b);
   }
 
   // Take every device buffer of this session from ``pool`` in stream order on the session's stream.

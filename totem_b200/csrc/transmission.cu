@@ -45,6 +45,23 @@ __device__ __forceinline__ float lobato5(const float* c, float g2) {
   return f;
 }
 
+// Form factor of one neutral (kind 0) or ionic (kind 1) coefficient row at s^2: real part fr
+// (Peng: occ * sum a_i exp(-b_i s^2); Lobato: occ * sum a_i (2 + b_i g^2) / (1 + b_i g^2)^2 *
+// exp(-B s^2), g^2 = 4 s^2; ionic rows mix the ion and atom sums by their fractions) and the
+// absorptive imaginary part fi (occ * Peng sum of the absorptive row, or 0).
+__device__ __forceinline__ void row_form(int kind, int lobato, const float* cf, const float* absorp, float s2,
+                                         float& fr, float& fi) {
+  if (kind == 0) {
+    if (lobato) fr = cf[0] * lobato5(cf + 1, 4.f * s2) * __expf(-cf[11] * s2);
+    else fr = cf[0] * peng5(cf + 1, s2);
+  } else {
+    if (lobato)
+      fr = cf[0] * (cf[1] * lobato5(cf + 2, 4.f * s2) + cf[12] * lobato5(cf + 13, 4.f * s2)) * __expf(-cf[23] * s2);
+    else fr = cf[0] * (cf[1] * peng5(cf + 2, s2) + cf[12] * peng5(cf + 13, s2));
+  }
+  fi = absorp != nullptr ? cf[0] * peng5(absorp, s2) : 0.f;
+}
+
 // exp(-2 pi i t) for t given in FP64, reduced to [0, 1) before the FP32 evaluation.
 __device__ __forceinline__ float2 phase_of(double t) {
   const double fr = t - floor(t);
@@ -104,16 +121,8 @@ __device__ void accumulate_rows(const TxGrid& g, const AtomRowsDev& rows, int ki
         if (SEP) ph = cmul(ex, sm.ey[a][ty * TX_PR + i]);
         else ph = phase_of(kxv[i] * sm.pos[a][0] + kyv[i] * sm.pos[a][1]);
         float fr, fi = 0.f;
-        if (kind == 0) {
-          if (g.lobato) fr = cf[0] * lobato5(cf + 1, 4.f * s2) * __expf(-cf[11] * s2);
-          else fr = cf[0] * peng5(cf + 1, s2);
-          if (rows.absorp != nullptr) fi = cf[0] * peng5(sm.absorp[a], s2);
-        } else if (kind == 1) {
-          if (g.lobato)
-            fr = cf[0] * (cf[1] * lobato5(cf + 2, 4.f * s2) + cf[12] * lobato5(cf + 13, 4.f * s2)) *
-                 __expf(-cf[23] * s2);
-          else fr = cf[0] * (cf[1] * peng5(cf + 2, s2) + cf[12] * peng5(cf + 13, s2));
-          if (rows.absorp != nullptr) fi = cf[0] * peng5(sm.absorp[a], s2);
+        if (kind <= 1) {
+          row_form(kind, g.lobato, cf, rows.absorp != nullptr ? sm.absorp[a] : nullptr, s2, fr, fi);
         } else if (kind == 2) {
           const int idx = (int)cf[2] - 1;
           const float m = (idx >= 0 && idx < g.cim_len && pix[i] >= 0) ? g.cim[idx * plane + pix[i]] : 0.f;
@@ -136,7 +145,7 @@ __device__ void accumulate_rows(const TxGrid& g, const AtomRowsDev& rows, int ki
 
 template <bool SEP>
 __global__ void __launch_bounds__(256) k_tx_structure(TxGrid g, AtomRowsDev nr, AtomRowsDev ir, AtomRowsDev cn,
-                                                      AtomRowsDev ci, float2* __restrict__ out) {
+                                                      AtomRowsDev ci, float2* __restrict__ out, int accumulate) {
   __shared__ TxSmem sm;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int slice = blockIdx.z;
@@ -165,8 +174,110 @@ __global__ void __launch_bounds__(256) k_tx_structure(TxGrid g, AtomRowsDev nr, 
   for (int i = 0; i < TX_PR; ++i) {
     if (pix[i] < 0) continue;
     const float ap = (g.aper_true != nullptr) ? g.aper_true[pix[i]] : 1.f;
-    dst[pix[i]] = cscale(acc[i], g.parameter * ap);
+    float2 v = cscale(acc[i], g.parameter * ap);
+    if (accumulate) v = cadd(dst[pix[i]], v);
+    dst[pix[i]] = v;
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// By species.  A 256-thread block owns a 64 x 64 pixel tile of one slice; thread (tx, ty) owns the
+// 16 pixels (r_tile + ty + 16 i, c_tile + tx + 16 j).  Per species the block accumulates
+//   S(r, c) = sum_atoms ey_a(r) * ex_a(c),  ex_a(c) = exp(-2 pi i kx(c) x_a), ey_a(r) likewise,
+// a complex rank-K update from per-atom tables staged in shared memory (16 atoms at a time),
+// then adds f_species(s^2) * S.  Table entries are stored so that one complex multiply-add is two
+// packed FMAs: ex as (re, im, -im, re), ey as (re, re, im, im).
+// ---------------------------------------------------------------------------------------------
+constexpr int SP_T = 64;
+constexpr int SP_CH = 16;
+
+struct SpSmem {
+  double pos[SP_CH][2];
+  float4 ex[SP_CH][SP_T];
+  float4 ey[SP_CH][SP_T];
+};
+
+__global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesDev nr, SpeciesDev ir,
+                                                        float2* __restrict__ out) {
+  __shared__ SpSmem sm;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int slice = blockIdx.z;
+  const int c_tile = blockIdx.x * SP_T, r_tile = blockIdx.y * SP_T;
+  float2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
+  for (int kind = 0; kind < 2; ++kind) {
+    const SpeciesDev& d = kind ? ir : nr;
+    if (d.seg_beg == nullptr) continue;
+    const int s_end = d.seg_beg[slice + 1];
+    for (int sidx = d.seg_beg[slice]; sidx < s_end; ++sidx) {
+      const int sp = d.seg[3 * sidx], a_begin = d.seg[3 * sidx + 1], a_end = d.seg[3 * sidx + 2];
+      float2 S[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) S[i][j] = make_float2(0.f, 0.f);
+      for (int a0 = a_begin; a0 < a_end; a0 += SP_CH) {
+        const int na = min(SP_CH, a_end - a0);
+        __syncthreads();  // previous chunk's tables fully read
+        if (threadIdx.x < 2 * na) sm.pos[threadIdx.x >> 1][threadIdx.x & 1] = d.pos[(long)a0 * 2 + threadIdx.x];
+        __syncthreads();
+        for (int e = threadIdx.x; e < na * 2 * SP_T; e += blockDim.x) {
+          const int a = e / (2 * SP_T), k = e - a * (2 * SP_T);
+          if (k < SP_T) {
+            const int cc = min(c_tile + k, g.p_w - 1);
+            const float2 p = phase_of(g.kx_axis[cc] * sm.pos[a][0]);
+            sm.ex[a][k] = make_float4(p.x, p.y, -p.y, p.x);
+          } else {
+            const int rr = min(r_tile + k - SP_T, g.p_h - 1);
+            const float2 p = phase_of(g.ky_axis[rr] * sm.pos[a][1]);
+            sm.ey[a][k - SP_T] = make_float4(p.x, p.x, p.y, p.y);
+          }
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int a = 0; a < na; ++a) {
+          float4 exv[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) exv[j] = sm.ex[a][tx + 16 * j];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float4 ey = sm.ey[a][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              S[i][j] = __ffma2_rn(make_float2(ey.x, ey.y), make_float2(exv[j].x, exv[j].y), S[i][j]);
+              S[i][j] = __ffma2_rn(make_float2(ey.z, ey.w), make_float2(exv[j].z, exv[j].w), S[i][j]);
+            }
+          }
+        }
+      }
+      const float* cf = d.coef + (long)sp * d.ncoef;
+      const float* ab = d.absorp != nullptr ? d.absorp + (long)sp * 10 : nullptr;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int r = min(r_tile + ty + 16 * i, g.p_h - 1), c = min(c_tile + tx + 16 * j, g.p_w - 1);
+          float fr, fi;
+          row_form(kind, g.lobato, cf, ab, __ldg(g.s2 + (long)r * g.p_w + c), fr, fi);
+          acc[i][j].x = fmaf(fr, S[i][j].x, fmaf(-fi, S[i][j].y, acc[i][j].x));
+          acc[i][j].y = fmaf(fr, S[i][j].y, fmaf(fi, S[i][j].x, acc[i][j].y));
+        }
+    }
+  }
+  float2* dst = out + (long)slice * g.p_h * g.p_w;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r_tile + ty + 16 * i, c = c_tile + tx + 16 * j;
+      if (r >= g.p_h || c >= g.p_w) continue;
+      const long pix = (long)r * g.p_w + c;
+      const float ap = (g.aper_true != nullptr) ? g.aper_true[pix] : 1.f;
+      dst[pix] = cscale(acc[i][j], g.parameter * ap);
+    }
 }
 
 // In-place inverse FFT of rows of length N (RowCfg<N>::G rows per CTA).
@@ -263,12 +374,22 @@ Status cols_exp(float2* data, int slices, int p_w, const float2* tw, float sig, 
 bool fused_fft_size_ok(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; }
 
 Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const AtomRowsDev& ion,
-                           const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out, cudaStream_t st) {
+                           const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out, cudaStream_t st,
+                           bool accumulate) {
   dim3 grid((g.p_w + TX_TC - 1) / TX_TC, (g.p_h + TX_TR - 1) / TX_TR, g.slices);
   if (g.slices == 0) return Status::Ok();
-  if (g.separable) k_tx_structure<true><<<grid, 256, 0, st>>>(g, neutral, ion, corr_n, corr_i, out);
-  else k_tx_structure<false><<<grid, 256, 0, st>>>(g, neutral, ion, corr_n, corr_i, out);
+  if (g.separable) k_tx_structure<true><<<grid, 256, 0, st>>>(g, neutral, ion, corr_n, corr_i, out, accumulate);
+  else k_tx_structure<false><<<grid, 256, 0, st>>>(g, neutral, ion, corr_n, corr_i, out, accumulate);
   return cuda_status(cudaGetLastError(), "k_tx_structure");
+}
+
+Status launch_tx_species(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, float2* out,
+                         cudaStream_t st) {
+  if (g.slices == 0) return Status::Ok();
+  if (!g.separable) return Status::Err(TOTEM_ERR_UNSUPPORTED, "species builder needs separable reciprocal grids");
+  dim3 grid((g.p_w + SP_T - 1) / SP_T, (g.p_h + SP_T - 1) / SP_T, g.slices);
+  k_tx_species<<<grid, 256, 0, st>>>(g, neutral, ion, out);
+  return cuda_status(cudaGetLastError(), "k_tx_species");
 }
 
 Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sig, const float2* tw_w,

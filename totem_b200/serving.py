@@ -129,19 +129,27 @@ def main(argv=None):
     ap.add_argument("--max-probes", type=int, default=1024)
     ap.add_argument("--slices", type=int, nargs=2, default=[20, 100])
     ap.add_argument("--rate", type=float, default=0.0,
-                    help="Poisson arrival rate (requests/s); 0 = 70%% of the measured burst capacity")
+                    help="Poisson arrival rate (requests/s); 0 = 70%% of the slower measured burst capacity")
     ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
+    ap.add_argument("--wave-mib", type=int, default=0, help="wave memory of the server (0 = its default)")
     ap.add_argument("--compare", action="store_true", help="also serve one request at a time")
     ns = ap.parse_args(argv)
     policy = capi.SCHED_SHORTEST if ns.policy == "shortest" else capi.SCHED_FIFO
     reqs = make_workload(ns.requests, ns.seed, tuple(ns.sizes), ns.max_probes, tuple(ns.slices))
+    kw = {"wave_bytes": ns.wave_mib << 20} if ns.wave_mib else {}
     # warm-up (kernels, pools) on a few requests, then the burst capacity
-    serve(reqs[:4], np.zeros(4), policy)
-    res_b, lat_b, mk_b = serve(reqs, np.zeros(len(reqs)), policy)
+    serve(reqs[:4], np.zeros(4), policy, **kw)
+    res_b, lat_b, mk_b = serve(reqs, np.zeros(len(reqs)), policy, **kw)
     out = [summary("burst", reqs, lat_b, mk_b)]
-    rate = ns.rate or 0.7 * len(reqs) / mk_b
+    slowest = mk_b
+    if ns.compare:
+        _, lat_sb, mk_sb = serve_one_at_a_time(reqs, np.zeros(len(reqs)))
+        out.append(summary("one-at-a-time burst", reqs, lat_sb, mk_sb))
+        slowest = max(mk_b, mk_sb)
+    # offered load: 70 % of the slower system's burst capacity
+    rate = ns.rate or 0.7 * len(reqs) / slowest
     arr = poisson_arrivals(len(reqs), rate, ns.seed)
-    res_p, lat_p, mk_p = serve(reqs, arr, policy)
+    res_p, lat_p, mk_p = serve(reqs, arr, policy, **kw)
     out.append(dict(summary("poisson", reqs, lat_p, mk_p), rate_hz=rate))
     if ns.compare:
         res_s, lat_s, mk_s = serve_one_at_a_time(reqs, arr)
