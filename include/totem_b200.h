@@ -254,6 +254,18 @@ typedef struct TotemRequestInfo {
   long long probe_slices;        /* w_num * depth * slices                                     */
 } TotemRequestInfo;
 
+/* Scheduler counters since totem_server_create. */
+typedef struct TotemServerStats {
+  long long ticks;               /* slice steps issued                                          */
+  long long probe_slices;        /* probe-slices advanced by them                                */
+  long long launches;            /* kernels the tick loop launched                               */
+  long long groups;              /* probe groups started                                         */
+  long long requests_done;
+  double issue_ms;               /* scheduler thread time spent issuing ticks                    */
+  double throttle_ms;            /* ... waiting for the device (ticks_ahead ticks in flight)     */
+  double idle_ms;                /* ... with nothing to run                                      */
+} TotemServerStats;
+
 TOTEM_API int totem_server_create(const TotemServerOptions *opt, totem_server **out);
 /* Validates the request (same checks and codes as totem_stem_run) and queues it. */
 TOTEM_API int totem_server_submit(totem_server *s, const TotemStemArgs *args, TotemStemOut *out,
@@ -262,6 +274,7 @@ TOTEM_API int totem_server_submit(totem_server *s, const TotemStemArgs *args, To
  * (TOTEM_ERR_TIMEOUT; timeout_ms < 0 waits without limit). */
 TOTEM_API int totem_server_wait(totem_server *s, unsigned long long ticket, int timeout_ms);
 TOTEM_API int totem_server_info(totem_server *s, unsigned long long ticket, TotemRequestInfo *info);
+TOTEM_API int totem_server_stats(totem_server *s, TotemServerStats *stats);
 /* Finishes every queued request, then releases the device state. */
 TOTEM_API int totem_server_destroy(totem_server *s);
 

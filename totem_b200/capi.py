@@ -72,6 +72,15 @@ class TotemRequestInfo(C.Structure):
                 ("run_ms", C.c_double), ("latency_ms", C.c_double), ("probe_slices", C.c_longlong)]
 
 
+class TotemServerStats(C.Structure):
+    _fields_ = [("ticks", C.c_longlong), ("probe_slices", C.c_longlong), ("launches", C.c_longlong),
+                ("groups", C.c_longlong), ("requests_done", C.c_longlong), ("issue_ms", C.c_double),
+                ("throttle_ms", C.c_double), ("idle_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TotemError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"totem_b200 error {code}: {msg}")
@@ -116,13 +125,14 @@ def load() -> C.CDLL:
     lib.totem_server_wait.argtypes = [vp, ull, C.c_int]
     lib.totem_server_info.argtypes = [vp, ull, C.POINTER(TotemRequestInfo)]
     lib.totem_server_destroy.argtypes = [vp]
+    lib.totem_server_stats.argtypes = [vp, C.POINTER(TotemServerStats)]
     lib.totem_plan_simulate.argtypes = [C.c_int, _ip, C.POINTER(C.c_longlong), _ip, _ip, ull, ull, C.c_int, _ip, _ip,
                                         ullp]
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
                  "totem_session_download", "totem_session_timing", "totem_session_transmission",
                  "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
-                 "totem_plan_simulate"):
+                 "totem_server_stats", "totem_plan_simulate"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -321,6 +331,11 @@ class Server:
         i = TotemRequestInfo()
         check(self.lib.totem_server_info(self.h, ticket, C.byref(i)))
         return i
+
+    def stats(self) -> dict:
+        st = TotemServerStats()
+        check(self.lib.totem_server_stats(self.h, C.byref(st)))
+        return st.as_dict()
 
     def close(self):
         if self.h:

@@ -121,6 +121,7 @@ struct totem_server {
   char* d_stage = nullptr;                           // device [K][slot_bytes]
   std::vector<cudaEvent_t> tick_ev;
   size_t max_groups = 4096;
+  TotemServerStats stats{};  // guarded by mu
 
   Status init();
   void prep_loop();
@@ -283,7 +284,10 @@ Status totem_server::complete_request(Request* r) {
 Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progressed) {
   *progressed = false;
   const int slot = tick % K;
+  const Clock::time_point t0 = Clock::now();
   TOTEM_CUDA(cudaEventSynchronize(tick_ev[slot]));  // tick - K has finished: its staging slot is free
+  const Clock::time_point t1 = Clock::now();
+  long long launched = 0, advanced = 0;
   // start the admitted groups
   std::vector<totem::PlanGroup> started = planner.start(tick);
   for (const totem::PlanGroup& g : started) {
@@ -302,6 +306,7 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
   const std::vector<totem::PlanGroup>& act = planner.active();
   if (act.empty()) return Status::Ok();
   *progressed = true;
+  for (const totem::PlanGroup& g : act) advanced += g.items;
   // one row and one column launch per window size over every active group
   std::map<int, std::vector<const totem::PlanGroup*>> by_n;
   for (const totem::PlanGroup& g : act) by_n[g.n].push_back(&g);
@@ -358,6 +363,7 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
     const auto* dib = reinterpret_cast<const int*>(d + ib_off);
     TOTEM_TRY(totem::launch_row_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
     TOTEM_TRY(totem::launch_col_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
+    launched += 2;
   }
   // groups that ran their last slice: detector sums, then their wave memory goes back
   for (const totem::PlanGroup& g : planner.finish(tick)) {
@@ -373,12 +379,20 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
       TOTEM_TRY(totem::launch_det_reduce(static_cast<const double*>(g.part) + e * estride, r->nblk, s->aper_num,
                                          g.items, (int)g.item0, s->depth,
                                          s->acc.as<double>() + (size_t)e * s->w_num * ad, sst));
+    launched += r->de.n_events;
     TOTEM_CUDA(cudaFreeAsync(g.psi, sst));
     TOTEM_CUDA(cudaFreeAsync(g.part, sst));
     r->items_left -= g.items;
     if (r->items_left == 0) TOTEM_TRY(complete_request(r));
   }
   TOTEM_CUDA(cudaEventRecord(tick_ev[slot], sst));
+  std::lock_guard<std::mutex> lk(mu);
+  stats.ticks += 1;
+  stats.probe_slices += advanced;
+  stats.launches += launched;
+  stats.groups += (long long)started.size();
+  stats.throttle_ms += ms_between(t0, t1);
+  stats.issue_ms += ms_between(t1, Clock::now());
   return Status::Ok();
 }
 
@@ -390,7 +404,9 @@ void totem_server::sched_loop() {
     std::vector<Request*> fresh;
     {
       std::unique_lock<std::mutex> lk(mu);
+      const Clock::time_point w0 = Clock::now();
       cv.wait(lk, [&] { return !ready.empty() || !planner.idle() || (stopping && prep_exited) || !fatal.ok(); });
+      stats.idle_ms += ms_between(w0, Clock::now());
       if (!fatal.ok()) break;
       if (ready.empty() && planner.idle() && stopping && prep_exited) break;
       while (!ready.empty()) {
@@ -461,6 +477,7 @@ void totem_server::done_loop() {
       }
     std::lock_guard<std::mutex> lk(mu);
     static_used -= r->reserve;
+    stats.requests_done += 1;
     if (st.ok()) {
       r->state = TOTEM_REQ_DONE;
       r->status = TOTEM_OK;
@@ -602,6 +619,13 @@ int totem_server_info(totem_server* s, unsigned long long ticket, TotemRequestIn
   if (done) info->latency_ms = ms_between(r->t_submit, r->t_done);
   info->probe_slices = (long long)r->args.w_num * r->args.depth * r->args.slices;
   if (r->state == TOTEM_REQ_FAILED) totem::set_last_error(r->error);
+  return TOTEM_OK;
+}
+
+int totem_server_stats(totem_server* s, TotemServerStats* out) {
+  if (!s || !out) return server_fail(Status::Err(TOTEM_ERR_INVALID_ARG, "NULL argument"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
   return TOTEM_OK;
 }
 

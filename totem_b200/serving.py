@@ -129,7 +129,8 @@ def main(argv=None):
     ap.add_argument("--max-probes", type=int, default=1024)
     ap.add_argument("--slices", type=int, nargs=2, default=[20, 100])
     ap.add_argument("--rate", type=float, default=0.0,
-                    help="Poisson arrival rate (requests/s); 0 = 70%% of the slower measured burst capacity")
+                    help="Poisson arrival rate (requests/s); 0 = --load times the server's burst capacity")
+    ap.add_argument("--load", type=float, default=0.85, help="offered load as a fraction of burst capacity")
     ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
     ap.add_argument("--wave-mib", type=int, default=0, help="wave memory of the server (0 = its default)")
     ap.add_argument("--compare", action="store_true", help="also serve one request at a time")
@@ -141,13 +142,10 @@ def main(argv=None):
     serve(reqs[:4], np.zeros(4), policy, **kw)
     res_b, lat_b, mk_b = serve(reqs, np.zeros(len(reqs)), policy, **kw)
     out = [summary("burst", reqs, lat_b, mk_b)]
-    slowest = mk_b
     if ns.compare:
         _, lat_sb, mk_sb = serve_one_at_a_time(reqs, np.zeros(len(reqs)))
         out.append(summary("one-at-a-time burst", reqs, lat_sb, mk_sb))
-        slowest = max(mk_b, mk_sb)
-    # offered load: 70 % of the slower system's burst capacity
-    rate = ns.rate or 0.7 * len(reqs) / slowest
+    rate = ns.rate or ns.load * len(reqs) / mk_b
     arr = poisson_arrivals(len(reqs), rate, ns.seed)
     res_p, lat_p, mk_p = serve(reqs, arr, policy, **kw)
     out.append(dict(summary("poisson", reqs, lat_p, mk_p), rate_hz=rate))

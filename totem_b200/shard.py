@@ -1,7 +1,7 @@
 """Spreading STEM work over ranks (one process per GPU) and collecting the detector images.
 
-The work units of the path are independent: scan positions, defocus-spread
-probes and frozen-phonon configurations.  Two ways to use several GPUs:
+The work units of the path are independent: scan positions, defocus-spread probes and
+frozen-phonon configurations.  Two ways to use several GPUs:
 
   * ``stem_sharded``: one request, its scan rows cut into contiguous bands, one band per rank.
     Each rank builds its own transmission from the atom list (no bulk data crosses NVLink) and
