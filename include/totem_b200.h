@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define TOTEM_ABI_VERSION 1
+#define TOTEM_ABI_VERSION 2
 
 /* Status codes.  The reference returns silently or aborts MATLAB (waveCuda.cpp:7-16,
  * cuda_source_lobato.cu:1253-1256); every entry point here returns one of these instead. */
@@ -107,6 +107,13 @@ typedef struct TotemStemOut {
   double *potential_im;
 } TotemStemOut;
 
+/* Storage of the transmission stack read by the slice loop. */
+enum {
+  TOTEM_T_COMPLEX64 = 0,         /* FP32 re/im (the reference's layout)                          */
+  TOTEM_T_BF16 = 1               /* bfloat16 re/im: half the bytes per slice, ~3 significant digits;
+                                    a precision trial, outside the 1e-4 parity bound            */
+};
+
 /* Engine options of one run (defaults: all zero). */
 typedef struct TotemRunOptions {
   int path;                        /* TOTEM_PATH_*                                              */
@@ -117,6 +124,7 @@ typedef struct TotemRunOptions {
                                       L2, 16-column tiles up to N = 512), 2 = propagator prefetched
                                       to shared memory, 3 = 80-register cap (more resident CTAs),
                                       5 = 8-column tiles, 6 = 32-column tiles (N <= 512)           */
+  int t_storage;                   /* TOTEM_T_* (fused path only)                                */
 } TotemRunOptions;
 
 /* Device times (CUDA events) of the last run, milliseconds. */
@@ -193,6 +201,38 @@ TOTEM_API int totem_stem_slices_noalloc(const void *transmission, int p_height, 
                                         const void *probe, int w_num, const void *propagator, const float *masks,
                                         int aper_num, int n, int step, int begin_row, int begin_col, int width_red,
                                         int depth, int item0, int items, double *result, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * HRTEM: plane-wave multislice over the whole potential grid, exit wave and partially coherent
+ * image.  The reference builds the transmission with the *P MEX and runs this part in MATLAB
+ * (ToTEM_submit_v1.m:1259-1369):  psi = incident wave;  per slice  psi = ifft2(fft2(psi .* T_k)
+ * .* psf_fft);  exit wave = psi;  image = sum_k gfsf_k |ifft2(fft2(psi) .* tf_k)|^2 with
+ * tf_k = ifftshift(tcc_k .* aperture).  The grid must be square, a power of two in [64, 2048].
+ * ------------------------------------------------------------------------------------------- */
+typedef struct TotemHrtemArgs {
+  int struct_size;               /* sizeof(TotemHrtemArgs)                                     */
+  const double *wave_re;         /* incident wave [P_H][P_W]; both NULL = plane wave of 1      */
+  const double *wave_im;
+  const double *prop_re;         /* propagator psf_fft [P_H][P_W], FFT order (:1330-1334)      */
+  const double *prop_im;
+  int defoci;                    /* transfer functions of the image; 0 = exit wave only        */
+  const double *tf_re;           /* [defoci][P_H][P_W], FFT order                              */
+  const double *tf_im;
+  const double *weights;         /* [defoci] (gfsf)                                            */
+  int t_storage;                 /* TOTEM_T_*                                                  */
+} TotemHrtemArgs;
+
+typedef struct TotemHrtemOut {
+  double *exit_re;               /* [P_H][P_W] exit wave, or NULL                              */
+  double *exit_im;
+  double *image;                 /* [P_H][P_W] image, or NULL                                  */
+} TotemHrtemOut;
+
+/* HRTEM on the specimen uploaded to ``s`` (totem_session_upload; its transmission is built if
+ * the session has none).  Synchronous: the outputs are filled on return. */
+TOTEM_API int totem_session_hrtem(totem_session *s, const TotemHrtemArgs *h, TotemHrtemOut *out);
+/* One-shot HRTEM: the specimen fields of ``specimen`` (probe, window and detector fields unused). */
+TOTEM_API int totem_hrtem_run(const TotemStemArgs *specimen, const TotemHrtemArgs *h, TotemHrtemOut *out);
 
 /* ---------------------------------------------------------------------------------------------
  * Serving: a resident scheduler with continuous batching.  No counterpart in the reference,

@@ -35,10 +35,13 @@ Decisions where the reference's two implementations disagree (each noted where a
      mid-slice detectors only, as the CUDA code does (cuda_source_lobato.cu:1342-1356, 1421).
 
 Parity of this oracle is pinned against golden fixtures produced by this very code and by the
-physics invariants in ``tests/test_oracle.py``; the reference publishes no golden vectors and its
-MATLAB path cannot run here (no MATLAB runtime), so at the FFT boundary it is *parity unpinned*
-apart from the checks against the reference's own CUDA engine run on a GPU
-(``tests/test_reference_engine.py``).
+physics invariants in ``tests/test_oracle.py``; the reference publishes no golden vectors, its
+MATLAB path cannot run here (no MATLAB runtime) and its CUDA engine is not run (it frees
+uninitialised device pointers and races in its potential kernels), so at the FFT boundary the
+oracle is *parity unpinned*.
+
+HRTEM (``hrtem_exit_wave``, ``hrtem_image``) restates ToTEM_submit_v1.m:1320-1369; the incident
+wave may be given (a tilted plane wave), the default is the plane wave of ones.
 """
 from __future__ import annotations
 
@@ -240,9 +243,9 @@ def _origins(req):
 # HRTEM plane-wave multislice (ToTEM_submit_v1.m:1320-1369)
 # ----------------------------------------------------------------------------------------------
 
-def hrtem_exit_wave(T: np.ndarray, prop_half: np.ndarray) -> np.ndarray:
+def hrtem_exit_wave(T: np.ndarray, prop_half: np.ndarray, wave: np.ndarray | None = None) -> np.ndarray:
     """Plane wave through all slices on the full grid; ``prop_half`` is the 1/2-limited propagator."""
-    psi = np.ones(T.shape[1:], dtype=np.complex128)
+    psi = np.ones(T.shape[1:], dtype=np.complex128) if wave is None else np.asarray(wave, dtype=np.complex128)
     for k in range(T.shape[0]):
         psi = psi * T[k]
         psi = sfft.fft2(psi)

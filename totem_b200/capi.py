@@ -48,9 +48,21 @@ class TotemStemOut(C.Structure):
     _fields_ = [("result", _dp), ("mid_layer_mat", _dp), ("potential_re", _dp), ("potential_im", _dp)]
 
 
+T_COMPLEX64, T_BF16 = 0, 1
+
+
 class TotemRunOptions(C.Structure):
     _fields_ = [("path", C.c_int), ("batch", C.c_int), ("skip_transmission", C.c_int), ("profile", C.c_int),
-                ("col_variant", C.c_int)]
+                ("col_variant", C.c_int), ("t_storage", C.c_int)]
+
+
+class TotemHrtemArgs(C.Structure):
+    _fields_ = [("struct_size", C.c_int), ("wave_re", _dp), ("wave_im", _dp), ("prop_re", _dp), ("prop_im", _dp),
+                ("defoci", C.c_int), ("tf_re", _dp), ("tf_im", _dp), ("weights", _dp), ("t_storage", C.c_int)]
+
+
+class TotemHrtemOut(C.Structure):
+    _fields_ = [("exit_re", _dp), ("exit_im", _dp), ("image", _dp)]
 
 
 class TotemTiming(C.Structure):
@@ -116,6 +128,8 @@ def load() -> C.CDLL:
     lib.totem_session_timing.argtypes = [vp, C.POINTER(TotemTiming)]
     lib.totem_session_transmission.argtypes = [vp, C.POINTER(vp)]
     lib.totem_stem_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemRunOptions), C.POINTER(TotemStemOut)]
+    lib.totem_session_hrtem.argtypes = [vp, C.POINTER(TotemHrtemArgs), C.POINTER(TotemHrtemOut)]
+    lib.totem_hrtem_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemHrtemArgs), C.POINTER(TotemHrtemOut)]
     lib.totem_transmission_run.argtypes = [C.POINTER(TotemStemArgs), C.POINTER(TotemStemOut)]
     lib.totem_stem_slices_noalloc.argtypes = ([vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp] + [C.c_int] * 9
                                               + [vp, vp])
@@ -130,7 +144,8 @@ def load() -> C.CDLL:
                                         ullp]
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
                  "totem_session_download", "totem_session_timing", "totem_session_transmission",
-                 "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_server_create",
+                 "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_session_hrtem",
+                 "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate"):
         getattr(lib, name).restype = C.c_int
@@ -248,9 +263,15 @@ class Session:
         check(self.lib.totem_session_upload(self.h, C.byref(self._m.args)))
 
     def run(self, what: int = 0, path: int = PATH_FUSED, batch: int = 0, skip_transmission: bool = False,
-            profile: bool = False, col_variant: int = 0):
-        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile), col_variant)
+            profile: bool = False, col_variant: int = 0, t_storage: int = T_COMPLEX64):
+        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile), col_variant, t_storage)
         check(self.lib.totem_session_run(self.h, what, C.byref(o)))
+
+    def hrtem(self, spec, t_storage: int = T_COMPLEX64, exit_wave: bool = True, image: bool = True):
+        """HRTEM on the uploaded specimen (``totem_session_hrtem``): (exit wave, image)."""
+        h, out, ex, img = _hrtem_marshal(spec, self.req.p_height, self.req.p_width, t_storage, exit_wave, image)
+        check(self.lib.totem_session_hrtem(self.h, C.byref(h.args), C.byref(out)))
+        return ex(), img
 
     def download(self, want_transmission: bool = False):
         req = self.req
@@ -369,6 +390,54 @@ def plan_simulate(n, items, slices, arrive, wave_bytes: int, chunk_bytes: int = 
     return first, done, mx.value
 
 
+class _HrtemMarshalled:
+    """Keeps the numpy buffers referenced by a TotemHrtemArgs alive."""
+
+    def __init__(self, spec, t_storage):
+        self.keep = []
+
+        def k(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            self.keep.append(a)
+            return _ptr(a)
+        a = TotemHrtemArgs()
+        a.struct_size = C.sizeof(TotemHrtemArgs)
+        if spec.wave is not None:
+            a.wave_re, a.wave_im = k(spec.wave.real), k(spec.wave.imag)
+        a.prop_re, a.prop_im = k(spec.prop.real), k(spec.prop.imag)
+        if spec.tf is not None and len(spec.tf):
+            a.defoci = len(spec.tf)
+            a.tf_re, a.tf_im = k(spec.tf.real), k(spec.tf.imag)
+            a.weights = k(spec.weights)
+        a.t_storage = t_storage
+        self.args = a
+
+
+def _hrtem_marshal(spec, ph, pw, t_storage, exit_wave, image):
+    h = _HrtemMarshalled(spec, t_storage)
+    out = TotemHrtemOut()
+    ere = eim = img = None
+    if exit_wave:
+        ere, eim = np.zeros((ph, pw)), np.zeros((ph, pw))
+        out.exit_re, out.exit_im = _ptr(ere), _ptr(eim)
+    if image and spec.tf is not None and len(spec.tf):
+        img = np.zeros((ph, pw))
+        out.image = _ptr(img)
+
+    def ex():
+        return None if ere is None else ere + 1j * eim
+    return h, out, ex, img
+
+
+def hrtem_run(specimen, spec, t_storage: int = T_COMPLEX64, exit_wave: bool = True, image: bool = True):
+    """One-shot HRTEM (``totem_hrtem_run``): returns (exit wave [P_H, P_W] complex, image or None)."""
+    lib = load()
+    m = Marshalled(specimen, False)
+    h, out, ex, img = _hrtem_marshal(spec, specimen.p_height, specimen.p_width, t_storage, exit_wave, image)
+    check(lib.totem_hrtem_run(C.byref(m.args), C.byref(h.args), C.byref(out)))
+    return ex(), img
+
+
 def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
     """One-shot STEM call through ``totem_stem_run`` (host buffers in, host buffers out)."""
     lib = load()
@@ -376,7 +445,7 @@ def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
     res = np.zeros(req.aper_num * req.depth)
     mid = np.zeros(req.aper_num * req.depth * len(req.mid_layer))
     out = TotemStemOut(_ptr(res), _ptr(mid), None, None)
-    opt = TotemRunOptions(path, batch, 0, 0, 0)
+    opt = TotemRunOptions(path, batch, 0, 0, 0, T_COMPLEX64)
     check(lib.totem_stem_run(C.byref(m.args), C.byref(opt), C.byref(out)))
     return res, mid
 

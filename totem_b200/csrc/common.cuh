@@ -131,10 +131,12 @@ struct SliceLoopArgs {
   double* part_mid = nullptr;      // [items][A][nblk]
   double* part_exit = nullptr;
   int col_variant = 0;             // column-pass variant (multislice.cu, col_pass)
+  int t_bf16 = 0;                  // the transmission slices are bfloat16 pairs, not complex64
 };
 // Number of column tiles per item (detector partial sums per probe) of a column-pass variant.
 int col_blocks(int n, int variant = 0);
-Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st);
+// tslice: T[slice] as complex64, or bfloat16 pairs when a.t_bf16.
+Status launch_row_pass(const SliceLoopArgs& a, const void* tslice, bool first, cudaStream_t st);
 // flags: 1 = mid-slice detectors, 2 = exit detectors, 4 = final pass (no inverse transform)
 Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st);
 // Continuous batching: one launch advances groups of items of several requests, each group at
@@ -163,6 +165,13 @@ Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, 
 Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                          const float2* tw, cudaStream_t st);
 
+// HRTEM imaging from the exit-wave spectrum spec [N][N] (FFT order): the exit wave
+// IFFT2(spec)/N^2 (complex64), and the image sum_k w_k |IFFT2(spec .* tf_k)/N^2|^2 (float32).
+// work holds `planes` N x N complex64 planes.
+Status launch_exit_wave(int n, const float2* spec, float2* work, float2* out, const float2* tw, cudaStream_t st);
+Status launch_tcc_image(int n, const float2* spec, const float2* tf, int planes, const double* w, float2* work,
+                        float* out, const float2* tw, cudaStream_t st);
+
 // Sum the per-column-block partials in a fixed order: acc[(w*A + a)*depth + pos].
 Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth,
                          double* acc, cudaStream_t st);
@@ -186,5 +195,7 @@ Status launch_d2f2(const double* re, const double* im, float2* out, long n, cuda
 Status launch_d2f(const double* in, float* out, long n, cudaStream_t st);
 Status launch_shift_masks(const double* aper, float* out, int aper_num, int h, int w, int shift,
                           cudaStream_t st);
+// complex64 -> bfloat16 pairs (round to nearest even), the storage of the BF16 transmission trial.
+Status launch_to_bf16(const float2* in, void* out, long n, cudaStream_t st);
 
 }  // namespace totem

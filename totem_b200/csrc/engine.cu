@@ -197,6 +197,7 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
   cudaStream_t st = stream;
   uploaded = false;
   t_valid = false;
+  tb_valid = false;
   has_result = false;
 
   // coefficient rows
@@ -352,13 +353,33 @@ Status totem_session::build_transmission(int path, int* launches) {
     *launches += 2;
   }
   t_valid = true;
+  tb_valid = false;
   return Status::Ok();
 }
 
 // ---------------------------------------------------------------------------------------------
 // Slice loop
 // ---------------------------------------------------------------------------------------------
-Status totem_session::slice_loop(int path, int batch, int col_variant, int* launches, int* batch_used) {
+Status totem_session::transmission_for(int t_storage, const void** t, size_t* slice_bytes, int* launches) {
+  const size_t plane = (size_t)p_h * p_w;
+  if (t_storage == TOTEM_T_BF16) {
+    if (!tb_valid) {
+      TOTEM_TRY(Tb.ensure(plane * std::max(slices, 1) * 4));
+      TOTEM_TRY(totem::launch_to_bf16(T.as<float2>(), Tb.p, (long)(plane * slices), stream));
+      ++*launches;
+      tb_valid = true;
+    }
+    *t = Tb.p;
+    *slice_bytes = plane * 4;
+  } else {
+    *t = T.p;
+    *slice_bytes = plane * sizeof(float2);
+  }
+  return Status::Ok();
+}
+
+Status totem_session::slice_loop(int path, int batch, int col_variant, int t_storage, int* launches,
+                                 int* batch_used) {
   const long items_total = (long)w_num * depth;
   const long ad = (long)aper_num * depth;
   const int L = (int)mid_layer.size();
@@ -398,6 +419,13 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int* laun
   totem::ScanGeom geo{begin_row, begin_col, step, width_red, depth, p_w};
   const float2* Tp = T.as<float2>();
   const size_t plane = (size_t)p_h * p_w;
+  const void* Tslices = Tp;
+  size_t tslice_bytes = plane * sizeof(float2);
+  if (t_storage != TOTEM_T_COMPLEX64) {
+    if (!fused) return Status::Err(TOTEM_ERR_UNSUPPORTED, "bfloat16 transmission storage needs the fused path");
+    TOTEM_TRY(transmission_for(t_storage, &Tslices, &tslice_bytes, launches));
+  }
+  auto tslice = [&](int k) { return static_cast<const char*>(Tslices) + (size_t)k * tslice_bytes; };
 
   for (long item0 = 0; item0 < items_total; item0 += B) {
     const int items = (int)std::min<long>(B, items_total - item0);
@@ -408,8 +436,9 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int* laun
       s.tw = tw_n.as<float2>(); s.aper_num = aper_num;
       s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
       s.col_variant = col_variant;
+      s.t_bf16 = (t_storage == TOTEM_T_BF16);
       TOTEM_TRY(prof_begin());
-      TOTEM_TRY(totem::launch_row_pass(s, Tp, true, stream));
+      TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
       TOTEM_TRY(prof_end(0));
       ++*launches;
       for (int k = 0; k < slices; ++k) {
@@ -429,7 +458,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int* laun
         ++*launches;
         if (k < slices - 1) {
           TOTEM_TRY(prof_begin());
-          TOTEM_TRY(totem::launch_row_pass(s, Tp + (size_t)(k + 1) * plane, false, stream));
+          TOTEM_TRY(totem::launch_row_pass(s, tslice(k + 1), false, stream));
           TOTEM_TRY(prof_end(0));
           ++*launches;
         }
@@ -504,6 +533,90 @@ Status totem_session::combine_results(const totem::DetectionEvents& de, int* lau
   return Status::Ok();
 }
 
+// ---------------------------------------------------------------------------------------------
+// HRTEM
+// ---------------------------------------------------------------------------------------------
+Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
+  if (!uploaded) return Status::Err(TOTEM_ERR_STATE, "HRTEM before a successful upload");
+  if (hr == nullptr || hr->struct_size != (int)sizeof(TotemHrtemArgs))
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "TotemHrtemArgs missing or of another size");
+  if (!hr->prop_re || !hr->prop_im) return Status::Err(TOTEM_ERR_INVALID_ARG, "the propagator is required");
+  if ((hr->wave_re == nullptr) != (hr->wave_im == nullptr))
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "wave_re and wave_im must both be given or both be NULL");
+  if (hr->defoci < 0 || (hr->defoci > 0 && (!hr->tf_re || !hr->tf_im || !hr->weights)))
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "defoci > 0 needs tf_re, tf_im and weights");
+  if (hr->t_storage != TOTEM_T_COMPLEX64 && hr->t_storage != TOTEM_T_BF16)
+    return Status::Err(TOTEM_ERR_INVALID_ARG, "unknown transmission storage");
+  if (p_h != p_w || !is_pow2(p_h) || p_h < 64 || p_h > 2048 || slices < 1)
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "HRTEM needs a square power-of-two grid of 64..2048 and a slice");
+  TOTEM_CUDA(cudaSetDevice(device));
+  const int n = p_h;
+  const size_t vol = (size_t)n * n;
+  int launches = 0;
+  if (!t_valid) TOTEM_TRY(build_transmission(TOTEM_PATH_FUSED, &launches));
+  const void* Tslices = nullptr;
+  size_t tslice_bytes = 0;
+  TOTEM_TRY(transmission_for(hr->t_storage, &Tslices, &tslice_bytes, &launches));
+
+  std::vector<float2> wave(vol), prop(vol);
+  for (size_t i = 0; i < vol; ++i) {
+    wave[i] = hr->wave_re ? make_float2((float)hr->wave_re[i], (float)hr->wave_im[i]) : make_float2(1.f, 0.f);
+    prop[i] = make_float2((float)hr->prop_re[i], (float)hr->prop_im[i]);
+  }
+  TOTEM_TRY(upload(hr_wave, wave, stream));
+  TOTEM_TRY(upload(hr_prop, prop, stream));
+  TOTEM_TRY(psi.ensure(vol * sizeof(float2)));
+
+  totem::SliceLoopArgs s;
+  s.n = n; s.items = 1; s.item0 = 0;
+  s.geo = totem::ScanGeom{0, 0, 0, 1, 1, n};
+  s.p_h = n;
+  s.psi = psi.as<float2>(); s.probe = hr_wave.as<float2>(); s.prop = hr_prop.as<float2>();
+  s.tw = tw_pw.as<float2>();
+  s.aper_num = 0;
+  s.t_bf16 = (hr->t_storage == TOTEM_T_BF16);
+  auto tslice = [&](int k) { return static_cast<const char*>(Tslices) + (size_t)k * tslice_bytes; };
+  // psi = wave .* T_0, then per slice FFT2 .* psf_fft IFFT2 .* T_{k+1}; the last column pass keeps
+  // the spectrum FFT2(psi_{S-1} .* T) .* psf_fft, whose IFFT2 is the exit wave
+  TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
+  for (int k = 0; k < slices; ++k) {
+    TOTEM_TRY(totem::launch_col_pass(s, k == slices - 1 ? 4 : 0, stream));
+    if (k < slices - 1) TOTEM_TRY(totem::launch_row_pass(s, tslice(k + 1), false, stream));
+  }
+  const float2* spec = psi.as<float2>();
+  const bool want_exit = out && (out->exit_re || out->exit_im);
+  const bool want_img = out && out->image && hr->defoci > 0;
+  std::vector<float2> exit_h;
+  std::vector<float> img_h;
+  if (want_exit) {
+    TOTEM_TRY(hr_work.ensure(vol * sizeof(float2)));
+    TOTEM_TRY(hr_exit.ensure(vol * sizeof(float2)));
+    TOTEM_TRY(totem::launch_exit_wave(n, spec, hr_work.as<float2>(), hr_exit.as<float2>(), tw_pw.as<float2>(), stream));
+    exit_h.resize(vol);
+    TOTEM_CUDA(cudaMemcpyAsync(exit_h.data(), hr_exit.p, vol * sizeof(float2), cudaMemcpyDeviceToHost, stream));
+  }
+  if (want_img) {
+    const int K = hr->defoci;
+    std::vector<float2> tf((size_t)K * vol);
+    for (size_t i = 0; i < tf.size(); ++i) tf[i] = make_float2((float)hr->tf_re[i], (float)hr->tf_im[i]);
+    TOTEM_TRY(upload(hr_tf, tf, stream));
+    TOTEM_TRY(upload(hr_w, std::vector<double>(hr->weights, hr->weights + K), stream));
+    TOTEM_TRY(hr_work.ensure((size_t)K * vol * sizeof(float2)));
+    TOTEM_TRY(hr_img.ensure(vol * sizeof(float)));
+    TOTEM_TRY(totem::launch_tcc_image(n, spec, hr_tf.as<float2>(), K, hr_w.as<double>(), hr_work.as<float2>(),
+                                      hr_img.as<float>(), tw_pw.as<float2>(), stream));
+    img_h.resize(vol);
+    TOTEM_CUDA(cudaMemcpyAsync(img_h.data(), hr_img.p, vol * sizeof(float), cudaMemcpyDeviceToHost, stream));
+  }
+  TOTEM_CUDA(cudaStreamSynchronize(stream));
+  for (size_t i = 0; i < exit_h.size(); ++i) {
+    if (out->exit_re) out->exit_re[i] = exit_h[i].x;
+    if (out->exit_im) out->exit_im[i] = exit_h[i].y;
+  }
+  for (size_t i = 0; i < img_h.size(); ++i) out->image[i] = img_h[i];
+  return Status::Ok();
+}
+
 Status totem_session::run(int what, const TotemRunOptions* opt) {
   if (!uploaded) return Status::Err(TOTEM_ERR_STATE, "run before a successful upload");
   TotemRunOptions o{};
@@ -524,7 +637,9 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
   TOTEM_CUDA(cudaEventRecord(ev[1], stream));
   if (what == 0) {
     if (!stem_ready && depth > 0) return Status::Err(TOTEM_ERR_STATE, "no STEM inputs uploaded");
-    TOTEM_TRY(slice_loop(o.path, o.batch, o.col_variant, &launches, &batch_used));
+    if (o.t_storage != TOTEM_T_COMPLEX64 && o.t_storage != TOTEM_T_BF16)
+      return Status::Err(TOTEM_ERR_INVALID_ARG, "unknown transmission storage");
+    TOTEM_TRY(slice_loop(o.path, o.batch, o.col_variant, o.t_storage, &launches, &batch_used));
   }
   else has_result = true;
   TOTEM_CUDA(cudaEventRecord(ev[2], stream));
@@ -747,6 +862,23 @@ int totem_session_transmission(totem_session* s, void** ptr) {
   if (!s->t_valid) return fail(Status::Err(TOTEM_ERR_STATE, "no transmission built"));
   *ptr = s->T.p;
   return TOTEM_OK;
+}
+
+int totem_session_hrtem(totem_session* s, const TotemHrtemArgs* h, TotemHrtemOut* out) {
+  if (!s) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "session is NULL"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  return guarded([&] { return s->hrtem(h, out); });
+}
+
+int totem_hrtem_run(const TotemStemArgs* specimen, const TotemHrtemArgs* h, TotemHrtemOut* out) {
+  return guarded([&]() -> Status {
+    totem_session* s = nullptr;
+    TOTEM_TRY(default_session(&s));
+    std::lock_guard<std::mutex> lk(s->mu);
+    TOTEM_CUDA(cudaSetDevice(s->device));
+    TOTEM_TRY(s->upload_args(specimen, false));
+    return s->hrtem(h, out);
+  });
 }
 
 int totem_stem_run(const TotemStemArgs* args, const TotemRunOptions* opt, TotemStemOut* out) {

@@ -14,6 +14,8 @@
 // Layout in HBM: psi[item][row][col] complex64, item = w * depth + pos (probe-major, as the
 // reference's w_series loop); T[slice][P_H][P_W]; H[N][N] and the masks [A][N][N] in natural
 // FFT order (the masks for the exit detector are ifftshift(aper), computed at upload).
+#include <cuda_bf16.h>
+
 #include <cmath>
 #include <vector>
 
@@ -25,12 +27,14 @@ namespace totem {
 namespace {
 
 // One CTA's share of a row pass: rows row0 .. row0+G-1 of one probe's wave.
-//   psi_item  the probe's wave [N][N];  t_origin  T at the window origin (row stride p_w);
-//   probe_item  the probe [N][N] (FIRST only: the first pass starts from the probe).
-template <int N, bool FIRST>
-__device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const float2* __restrict__ t_origin, long p_w,
+//   psi_item  the probe's wave [N][N];  t_origin  T at the window origin (row stride p_w),
+//   complex64 or, with TB16, bfloat16 pairs;  probe_item  the probe [N][N] (FIRST only: the first
+//   pass starts from the probe).
+template <int N, bool FIRST, bool TB16 = false>
+__device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const void* __restrict__ t_origin, long p_w,
                                          const float2* __restrict__ probe_item, int row0, float scale,
                                          const float2* __restrict__ tw) {
+  using TElem = std::conditional_t<TB16, __nv_bfloat162, float2>;
   constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
@@ -38,7 +42,7 @@ __device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const fl
   const int g = threadIdx.x / T, j = threadIdx.x - g * T;
   const int row = row0 + g;
   load_twiddles<N>(s_tw, tw);
-  const float2* __restrict__ trow = t_origin + (long)row * p_w;
+  const TElem* __restrict__ trow = static_cast<const TElem*>(t_origin) + (long)row * p_w;
   float2* prow = psi_item + (long)row * N;
   const RowLayout<N> L;
   const auto sync = group_sync<N>(g);
@@ -48,7 +52,10 @@ __device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const fl
   // reads only its own elements.
   auto prefetch_t = [&]() {
 #pragma unroll
-    for (int m = 0; m < P; ++m) cp_async8(&s_x[L.pos(g, j, m)], trow + j + m * T);
+    for (int m = 0; m < P; ++m) {
+      if constexpr (TB16) cp_async4(&s_x[L.pos(g, j, m)], trow + j + m * T);
+      else cp_async8(&s_x[L.pos(g, j, m)], trow + j + m * T);
+    }
     cp_async_commit();
   };
   float2 v[P];
@@ -65,25 +72,32 @@ __device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const fl
   if (!FIRST) fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync, prefetch_t);
   cp_async_wait_all();
 #pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = cscale(cmul(v[m], s_x[L.pos(g, j, m)]), scale);
+  for (int m = 0; m < P; ++m) {
+    float2 t;
+    if constexpr (TB16) t = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&s_x[L.pos(g, j, m)]));
+    else t = s_x[L.pos(g, j, m)];
+    v[m] = cscale(cmul(v[m], t), scale);
+  }
   sync();  // every thread of the transform has read its window values before the region is reused
   fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
   for (int m = 0; m < P; ++m) prow[j + m * T] = v[m];
 }
 
-template <int N, bool FIRST>
+template <int N, bool FIRST, bool TB16>
 __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
-    k_row_pass(SliceLoopArgs a, const float2* __restrict__ tslice, float scale) {
+    k_row_pass(SliceLoopArgs a, const void* __restrict__ tslice, float scale) {
   constexpr int G = RowCfg<N>::G;
+  using TElem = std::conditional_t<TB16, __nv_bfloat162, float2>;
   const long grow0 = (long)blockIdx.x * G;  // G divides N: the CTA's rows belong to one item
   const int item = (int)(grow0 / N), row0 = (int)(grow0 % N);
   const int gi = a.item0 + item;
   const int w = gi / a.geo.depth, pos = gi - w * a.geo.depth;
   const int x0 = a.geo.begin_row + (pos / a.geo.width_red) * a.geo.step;
   const int y0 = a.geo.begin_col + (pos % a.geo.width_red) * a.geo.step;
-  row_tile<N, FIRST>(a.psi + (long)item * N * N, tslice + (long)x0 * a.geo.p_width + y0, a.geo.p_width,
-                     a.probe + (long)w * N * N, row0, scale, a.tw);
+  row_tile<N, FIRST, TB16>(a.psi + (long)item * N * N,
+                           static_cast<const TElem*>(tslice) + (long)x0 * a.geo.p_width + y0, a.geo.p_width,
+                           a.probe + (long)w * N * N, row0, scale, a.tw);
 }
 
 // Deterministic block sum of one double per thread; result valid in thread 0.
@@ -281,15 +295,20 @@ __global__ void k_combine(const double* __restrict__ acc, const double* __restri
   out[i] = s;
 }
 
-template <int N, bool FIRST>
-Status row_pass(const SliceLoopArgs& a, const float2* tslice, cudaStream_t st) {
+template <int N, bool FIRST, bool TB16>
+Status row_pass_t(const SliceLoopArgs& a, const void* tslice, cudaStream_t st) {
   constexpr int G = RowCfg<N>::G, T = RowCfg<N>::T;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_row_pass<N, FIRST>, smem));
+  TOTEM_TRY(ensure_smem((const void*)k_row_pass<N, FIRST, TB16>, smem));
   const long rows = (long)a.items * N;
   const float scale = FIRST ? 1.f : 1.f / ((float)N * (float)N);
-  k_row_pass<N, FIRST><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale);
+  k_row_pass<N, FIRST, TB16><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale);
   return cuda_status(cudaGetLastError(), "k_row_pass");
+}
+
+template <int N, bool FIRST>
+Status row_pass(const SliceLoopArgs& a, const void* tslice, cudaStream_t st) {
+  return a.t_bf16 ? row_pass_t<N, FIRST, true>(a, tslice, st) : row_pass_t<N, FIRST, false>(a, tslice, st);
 }
 
 template <int N, bool PREFETCH, int CTAS128, int GW>
@@ -373,7 +392,7 @@ int col_blocks(int n, int variant) {
   return 0;
 }
 
-Status launch_row_pass(const SliceLoopArgs& a, const float2* tslice, bool first, cudaStream_t st) {
+Status launch_row_pass(const SliceLoopArgs& a, const void* tslice, bool first, cudaStream_t st) {
   switch (a.n) {
 #define TOTEM_ROW(NN) \
   case NN: return first ? row_pass<NN, true>(a, tslice, st) : row_pass<NN, false>(a, tslice, st);

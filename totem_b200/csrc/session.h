@@ -167,6 +167,10 @@ struct totem_session {
   // work buffers and results
   totem::DevBuf T, psi, part, acc, out_result, out_mid;
   totem::DevBuf ev_slice;  // device copy of DetectionEvents::event_of_slice (serving scheduler)
+  totem::DevBuf Tb;        // the transmission as bfloat16 pairs (TOTEM_T_BF16)
+  bool tb_valid = false;
+  // HRTEM inputs and outputs
+  totem::DevBuf hr_wave, hr_prop, hr_tf, hr_w, hr_work, hr_exit, hr_img;
   bool t_valid = false;
   bool has_result = false;
   int last_what = 0;
@@ -195,7 +199,7 @@ struct totem_session {
   void for_each_buf(F&& f) {
     for (totem::DevBuf* b : {&probe, &prop, &mask_mid, &mask_exit, &tw_n, &tw_pw, &tw_ph, &gfsf_d, &kx_axis, &ky_axis,
                              &kx, &ky, &s2, &aper_true, &cim, &T, &psi, &part, &acc, &out_result, &out_mid,
-                             &ev_slice})
+                             &ev_slice, &Tb, &hr_wave, &hr_prop, &hr_tf, &hr_w, &hr_work, &hr_exit, &hr_img})
       f(*b);
     for (totem::RowsDev* r : {&rows_n, &rows_i, &rows_cn, &rows_ci})
       for (totem::DevBuf* b : {&r->pos, &r->coef, &r->absorp, &r->beg}) f(*b);
@@ -253,7 +257,10 @@ struct totem_session {
   // Per-event detector sums acc[event][w][A][depth] -> out_result (exit) and out_mid (layers),
   // weighted by gfsf over w (accumulate_result, cuda_source_lobato.cu:981-1015).
   Status combine_results(const totem::DetectionEvents& de, int* launches);
-  Status slice_loop(int path, int batch, int col_variant, int* launches, int* batch_used);
+  Status slice_loop(int path, int batch, int col_variant, int t_storage, int* launches, int* batch_used);
+  // The transmission slices as the slice loop reads them (complex64, or bfloat16 pairs).
+  Status transmission_for(int t_storage, const void** t, size_t* slice_bytes, int* launches);
+  Status hrtem(const TotemHrtemArgs* h, TotemHrtemOut* out);
   Status run(int what, const TotemRunOptions* opt);
   Status collect_timing();
   Status download(TotemStemOut* out);

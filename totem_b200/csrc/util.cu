@@ -1,4 +1,6 @@
 // Status helpers and the small conversion kernels used while uploading a request.
+#include <cuda_bf16.h>
+
 #include <map>
 #include <mutex>
 #include <utility>
@@ -62,6 +64,11 @@ __global__ void k_shift_masks(const double* __restrict__ aper, float* __restrict
   }
 }
 
+__global__ void k_to_bf16(const float2* __restrict__ in, __nv_bfloat162* __restrict__ out, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = __float22bfloat162_rn(in[i]);
+}
+
 inline int grid_for(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 16); }
 
 }  // namespace
@@ -83,6 +90,12 @@ Status launch_shift_masks(const double* aper, float* out, int aper_num, int h, i
   if (n == 0) return Status::Ok();
   k_shift_masks<<<grid_for(n), 256, 0, st>>>(aper, out, aper_num, h, w, shift);
   return cuda_status(cudaGetLastError(), "k_shift_masks");
+}
+
+Status launch_to_bf16(const float2* in, void* out, long n, cudaStream_t st) {
+  if (n == 0) return Status::Ok();
+  k_to_bf16<<<grid_for(n), 256, 0, st>>>(in, static_cast<__nv_bfloat162*>(out), n);
+  return cuda_status(cudaGetLastError(), "k_to_bf16");
 }
 
 }  // namespace totem

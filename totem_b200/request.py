@@ -210,3 +210,84 @@ def with_absorption(req: StemRequest, seed: int = 1, scale: float = 0.05) -> Ste
         return c
     return replace(req, absorp_n=rows(len(req.ele_n)) if len(req.ele_n) else None,
                    absorp_n_i=rows(len(req.ele_n_i)) if len(req.ele_n_i) else None)
+
+
+# ----------------------------------------------------------------------------------------------
+# HRTEM (the reference's HRTEMsimulation: *P transmission, then plane-wave multislice and TCC
+# imaging in MATLAB, ToTEM_submit_v1.m:1259-1369)
+# ----------------------------------------------------------------------------------------------
+
+@dataclass
+class HrtemSpec:
+    """Inputs of the HRTEM step after the transmission."""
+    prop: np.ndarray                       # (P, P) complex psf_fft, FFT order
+    wave: Optional[np.ndarray] = None      # (P, P) incident wave; None = plane wave of ones
+    tf: Optional[np.ndarray] = None        # (K, P, P) complex, FFT order: ifftshift(tcc_k .* aperture)
+    weights: Optional[np.ndarray] = None   # (K,) gfsf
+
+
+def specimen_request(structure: specimen.Structure, flag: str, kv: float, sampling: float, p: int) -> StemRequest:
+    """Transmission-only request (the ``*P`` MEX inputs) of ``structure`` on a p x p grid."""
+    nuc, ion = specimen.potential_params(structure.atoms, flag)
+    ele_n, ele_n_i, series_n, series_n_i = specimen.slice_rows(
+        nuc, ion, structure.slice_dz, structure.slicethick, 0, flag, 0)
+    kx, ky, s2 = optics.reciprocal_grids(p, p, sampling)
+    S = structure.n_slices
+    return StemRequest(
+        param=flag, probe=np.zeros((1, 2, 2), dtype=np.complex128), aper=np.zeros((0, 2, 2)),
+        aper2=np.zeros((0, 2, 2)), ele_n=ele_n, series_n=series_n if len(series_n) else np.zeros(S),
+        ele_n_i=ele_n_i, series_n_i=series_n_i if len(series_n_i) else np.zeros(S),
+        kx=kx, ky=ky, s2=s2, prop=np.zeros((2, 2), dtype=np.complex128), gfsf=np.ones(1),
+        p_height=p, p_width=p, step=0, beginrow=0, begincol=0, width_red=0, hight_red=0,
+        sigma=optics.interaction_sigma(kv), parameter=optics.potential_parameter(p, p, sampling),
+        aper_true=np.ones((p, p)))
+
+
+def hrtem_spec(p: int, sampling: float, kv: float, dz: float, defocus_nm: float = 0.0, cs_mm: float = 0.0,
+               aperture_mrad: Optional[float] = None, focal_spread_nm: float = 0.0, focal_steps: int = 1,
+               image: bool = True) -> HrtemSpec:
+    """Propagator with the HRTEM half-Nyquist limit (ToTEM_submit_v1.m:1330-1334) and, for the
+    image, the transfer functions tf_k = ifftshift(tcc_k .* aperture) with their Gaussian focal
+    weights (WholeTCC2D_newTEM, Gaussian_focal)."""
+    prop = optics.propagator(p, sampling, kv, dz, "1/2")
+    if not image:
+        return HrtemSpec(prop=prop)
+    spec = optics.ProbeSpec(kv=kv, semi_angle_mrad=aperture_mrad or 100.0,
+                            aberrations=optics.Aberrations(focus=defocus_nm, Cs=cs_mm * 1e6),
+                            focal_spread_nm=focal_spread_nm, focal_steps=focal_steps)
+    tcc, w = optics.tcc_stack(spec, p, sampling)
+    ap = np.ones((p, p))
+    if aperture_mrad:
+        lam_a = optics.wavelength_nm(kv) * 10
+        ap = optics.aperture_mask(p, sampling, aperture_mrad * 1e-3 / lam_a)
+    tf = np.fft.ifftshift(tcc * ap, axes=(-2, -1))
+    return HrtemSpec(prop=prop, tf=tf, weights=np.asarray(w, dtype=np.float64))
+
+
+def build_si_hrtem_001(cells=(4, 4, 20), p: int = 256, kv: float = 200.0, flag: str = LOBATO,
+                       defocus_nm: float = -50.0, cs_mm: float = 1.2, aperture_mrad: float = 20.0,
+                       slices: Optional[int] = None):
+    """Si diamond [001], 4 x 4 x 20 cells, 256^2 (0.08486 Angstrom), 80 slices of 1.358
+    Angstrom, Lobato, 200 kV, plane wave; image with Cs 1.2 mm, defocus -50 nm, 20 mrad.
+    ``slices`` keeps only the first slices (small test cases).  Returns (specimen, HrtemSpec)."""
+    st = specimen.si_001(*cells)
+    if slices is not None:
+        st = specimen.Structure(st.atoms, st.extent, st.slice_dz, slices)
+    sampling = st.extent[0] / p
+    req = specimen_request(st, flag, kv, sampling, p)
+    return req, hrtem_spec(p, sampling, kv, st.slice_dz, defocus_nm, cs_mm, aperture_mrad)
+
+
+def build_si_hrtem_110(repeats: int = 520, p: int = 1024, sampling: float = 0.05, kv: float = 200.0,
+                       flag: str = LOBATO, defocus_nm: float = -50.0, cs_mm: float = 1.2,
+                       aperture_mrad: float = 20.0, focal_spread_nm: float = 4.0, focal_steps: int = 11):
+    """Si [110], ``repeats`` slices of a/sqrt2 (520: 200 nm), centred on a p x p grid; the image
+    over ``focal_steps`` Gaussian-weighted defoci of rms ``focal_spread_nm``."""
+    a = 5.431
+    field = p * sampling
+    nx, ny = max(1, int(field // a) - 1), max(1, int(field // (a / math.sqrt(2))) - 1)
+    st = specimen.center_in_field(specimen.si_110(nx, ny, repeats), field, field)
+    req = specimen_request(st, flag, kv, sampling, p)
+    return req, hrtem_spec(p, sampling, kv, st.slice_dz, defocus_nm, cs_mm, aperture_mrad, focal_spread_nm,
+                           focal_steps)
+
