@@ -12,10 +12,10 @@ import numpy as np
 
 
 class _DeviceArray:
-    """A raw device buffer seen through the CUDA array interface (read-only)."""
+    """A raw device buffer seen through the CUDA array interface (the tests only read it)."""
 
     def __init__(self, ptr: int, shape, typestr: str):
-        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), True),
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
                                          "version": 3, "strides": None}
 
 

@@ -137,7 +137,8 @@ struct SliceLoopArgs {
 int col_blocks(int n, int variant = 0);
 // tslice: T[slice] as complex64, or bfloat16 pairs when a.t_bf16.
 Status launch_row_pass(const SliceLoopArgs& a, const void* tslice, bool first, cudaStream_t st);
-// flags: 1 = mid-slice detectors, 2 = exit detectors, 4 = final pass (no inverse transform)
+// flags: 1 = mid-slice detectors, 2 = exit detectors, 4 = final pass (no inverse transform),
+// 8 = with 4, store the spectrum in psi
 Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st);
 // Continuous batching: one launch advances groups of items of several requests, each group at
 // its own slice (slice = tick - start_tick).  Items of a launch are numbered group by group;

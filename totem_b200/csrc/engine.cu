@@ -580,7 +580,7 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
   // the spectrum FFT2(psi_{S-1} .* T) .* psf_fft, whose IFFT2 is the exit wave
   TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
   for (int k = 0; k < slices; ++k) {
-    TOTEM_TRY(totem::launch_col_pass(s, k == slices - 1 ? 4 : 0, stream));
+    TOTEM_TRY(totem::launch_col_pass(s, k == slices - 1 ? 4 | 8 : 0, stream));
     if (k < slices - 1) TOTEM_TRY(totem::launch_row_pass(s, tslice(k + 1), false, stream));
   }
   const float2* spec = psi.as<float2>();

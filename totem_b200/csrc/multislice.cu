@@ -143,7 +143,7 @@ struct ColInputs {
 
 // One CTA's share of a column pass: columns cb*G .. cb*G+G-1 of one probe's wave.  ``item`` is
 // the item's index in the partial-sum arrays.  flags: 1 mid detectors, 2 exit detectors,
-// 4 final pass (no inverse transform).
+// 4 final pass (no inverse transform), 8 (with 4) store the spectrum.
 template <int N, bool PREFETCH, int G>
 __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const ColInputs& in, int item, int cb, int flags,
                                          const float2* __restrict__ tw) {
@@ -188,7 +188,13 @@ __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const Co
     if (flags & 1) detect<N>(inten, in.mask_mid, in.aper_num, j, c, in.part_mid, item, cb, nblk, red);
     if (flags & 2) detect<N>(inten, in.mask_exit, in.aper_num, j, c, in.part_exit, item, cb, nblk, red);
   }
-  if (flags & 4) return;
+  if (flags & 4) {
+    if (flags & 8) {  // keep the spectrum (HRTEM: the exit wave and image are taken from it)
+#pragma unroll
+      for (int m = 0; m < P; ++m) base[(long)(j + m * T) * N] = v[m];
+    }
+    return;
+  }
   fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
   for (int m = 0; m < P; ++m) base[(long)(j + m * T) * N] = v[m];
