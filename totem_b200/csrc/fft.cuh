@@ -299,6 +299,13 @@ struct SyncNamed {  // one named barrier per group of NT threads (NT a multiple 
 // One Stockham stage.  Register layout at stage input: v[q*R + r] = x[(j + q*T) + r*N/R];
 // for stage 0 that is the entry layout v[m] = x[j + m*T] permuted at compile time.
 // ---------------------------------------------------------------------------------------------
+// Derive the twiddles of a thread's later sub-sequences from the first by constant rotations
+// (fewer shared-memory loads, a few more FMAs); see StageLoop.
+#ifndef TOTEM_TW_DERIVE
+#define TOTEM_TW_DERIVE 1
+#endif
+constexpr bool kTwiddleDerive = TOTEM_TW_DERIVE != 0;
+
 template <int N, int S, bool INV, class Layout, class Sync, class Hook>
 struct StageLoop {
   __device__ __forceinline__ static void run(float2 (&v)[Fft<N>::P], int j, int g, const float2* __restrict__ tw,
@@ -318,19 +325,37 @@ struct StageLoop {
 #pragma unroll
       for (int m = 0; m < P; ++m) v[m] = t[m];
     }
+    if constexpr (kTwiddleDerive && Ns > 1 && Q > 1 && T * Q <= Ns) {
+      // The thread's sub-sequences are b = j + q*T < Ns, so their twiddles are
+      // W^(r (j + q T)) = W^(r j) * W^(r q T): one table load per r, and a compile-time rotation
+      // for q > 0 (one shared-memory load instead of Q).
+      const float2* twr = tw + StageInfo<N, S>::tw_off + j;
+      static_for<1, R>([&](auto rc) {
+        constexpr int r = decltype(rc)::value;
+        const float2 w = twr[(r - 1) * Ns];
+        static_for<0, Q>([&](auto qc) {
+          constexpr int q = decltype(qc)::value;
+          const float2 x = INV ? cmulc(v[q * R + r], w) : cmul(v[q * R + r], w);
+          v[q * R + r] = twiddle_const<r * q * T, Ns * R, INV>(x);
+        });
+      });
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int b = j + q * T;
-      if constexpr (Ns > 1) {
-        const int k = b % Ns;
-        const float2* twr = tw + StageInfo<N, S>::tw_off + k;
+      for (int q = 0; q < Q; ++q) dft_r<R, INV>(&v[q * R]);
+    } else {
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-          const float2 w = twr[(r - 1) * Ns];
-          v[q * R + r] = INV ? cmulc(v[q * R + r], w) : cmul(v[q * R + r], w);
+      for (int q = 0; q < Q; ++q) {
+        const int b = j + q * T;
+        if constexpr (Ns > 1) {
+          const int k = b % Ns;
+          const float2* twr = tw + StageInfo<N, S>::tw_off + k;
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            const float2 w = twr[(r - 1) * Ns];
+            v[q * R + r] = INV ? cmulc(v[q * R + r], w) : cmul(v[q * R + r], w);
+          }
         }
+        dft_r<R, INV>(&v[q * R]);
       }
-      dft_r<R, INV>(&v[q * R]);
     }
     if constexpr (LAST) {
       // outputs at b + r*N/R = j + T*(q + r*Q): back to v[m] = x[j + m*T]
