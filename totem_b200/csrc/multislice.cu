@@ -203,8 +203,12 @@ __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const Co
 // Column-pass variants, per 2048-probe launch on the SrTiO3 512^2 workload (microseconds per
 // probe): 16-column tiles with the propagator read from global memory (L2-resident) at a
 // 128-register cap, 0.98 (the default); 8-column tiles 1.11; 32-column tiles 1.32; 16-column
-// tiles at an 80-register cap 1.10.  With 8-column tiles, prefetching the propagator into shared
-// memory (4.6 ms against 4.3 ms per 4096 probes) and an 80-register cap (5.8 ms) were slower.
+// tiles at an 80-register cap 1.10 (it spills).  A persistent column pass streaming the next
+// tile into shared memory with cp.async while transforming the current one (one 256-thread CTA
+// per SM for its 134 KB of shared memory) measured 1.22, with 8-column tiles (3 CTAs per SM)
+// 1.24: the pass needs warps more than it needs its loads hidden.  With 8-column tiles,
+// prefetching the propagator into shared memory (4.6 ms against 4.3 ms per 4096 probes) and an
+// 80-register cap (5.8 ms) were slower.
 template <int N, bool PREFETCH, int CTAS128, int GW>
 __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
     k_col_pass(SliceLoopArgs a, int flags) {
