@@ -94,3 +94,30 @@ def test_precision_sweep_si110_520(engine_lib):
     print(json.dumps(rep))
     assert rep["fp32"]["image_rel_l2"] < 1e-3
     assert rep["fp32_bf16_t"]["image_rel_l2"] < 0.2
+
+
+def test_config1_full_size_vs_cpu_oracle(engine_lib):
+    """Si [001] 4x4x20 cells, 256^2, 80 slices, Lobato 200 kV, image at Cs 1.2 mm / -50 nm /
+    20 mrad: parity at full size and the GPU and CPU-oracle times of one simulation."""
+    import time
+    req, hs = request.build_si_hrtem_001()
+    capi.hrtem_run(req, hs)  # warm-up
+    gpu = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ex, img = capi.hrtem_run(req, hs)
+        gpu.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    rex, rimg = _oracle(req, hs)
+    cpu_s = time.perf_counter() - t0
+    rep = {"workload": "Si [001] 4x4x20 cells, 256^2, 80 slices, Lobato 200 kV, Cs 1.2 mm, df -50 nm, 20 mrad",
+           "gpu_s_median": float(np.median(gpu)), "cpu_oracle_s": cpu_s, "cpu_threads": 1,
+           "exit_rel_l2": rel_l2(ex, rex), "image_rel_l2": rel_l2(img, rimg),
+           "note": "GPU time is the whole totem_hrtem_run call from host arrays (upload, transmission, "
+                   "80 slices, exit wave, image, download)"}
+    out = os.environ.get("TOTEM_REPORT_DIR")
+    if out:
+        with open(os.path.join(out, "hrtem_si001_config1.json"), "w") as f:
+            json.dump(rep, f, indent=1)
+    print(json.dumps(rep))
+    assert rep["exit_rel_l2"] < TOL and rep["image_rel_l2"] < TOL

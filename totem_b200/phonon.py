@@ -15,6 +15,7 @@ from __future__ import annotations
 import argparse
 import json
 import time
+from dataclasses import replace
 
 import numpy as np
 
@@ -61,6 +62,8 @@ def main(argv=None):
     ap.add_argument("--window", type=int, default=1024)
     ap.add_argument("--cells", type=int, nargs=3, default=[8, 8, 50])
     ap.add_argument("--wave-gib", type=int, default=4)
+    ap.add_argument("--plain-sample", type=int, default=8,
+                    help="probes of one configuration timed through the per-probe cuFFT path (0 = skip)")
     ns = ap.parse_args(argv)
 
     def builder(phonon_seed):
@@ -79,12 +82,26 @@ def main(argv=None):
     t0 = time.perf_counter()
     res_s, mid_s = frozen_phonon_sequential(configs)
     t_s = time.perf_counter() - t0
+    plain = None
+    if ns.plain_sample:
+        # the reference's structure: one probe at a time through cuFFT (batch = 1), on a sample
+        sub = replace(configs[0], hight_red=1, width_red=ns.plain_sample)
+        sess = capi.Session()
+        sess.upload(sub)
+        sess.run(path=capi.PATH_PLAIN, batch=1)
+        t0 = time.perf_counter()
+        sess.run(path=capi.PATH_PLAIN, batch=1, skip_transmission=True)
+        sess.download()
+        plain = sub.probe_slices / (time.perf_counter() - t0)
+        sess.close()
     out = {"workload": f"SrTiO3 {ns.cells} frozen phonon, {ns.configs} configurations, "
                        f"{ns.raster}x{ns.raster} probes, window {ns.window}^2",
            "probe_slices": int(ps), "host_build_s": t_build,
            "batched_probe_slices_per_s": ps / t_b, "sequential_probe_slices_per_s": ps / t_s,
            "identical": bool(np.array_equal(res_b, res_s) and np.array_equal(mid_b, mid_s)),
-           "wave_gib": ns.wave_gib, "server": stats}
+           "wave_gib": ns.wave_gib, "server": stats,
+           "plain_per_probe_probe_slices_per_s": plain,
+           "plain_sample": f"{ns.plain_sample} probes of configuration 0, batch 1, transmission built beforehand"}
     print(json.dumps(out), flush=True)
     return out
 
