@@ -235,6 +235,29 @@ TOTEM_API int totem_session_hrtem(totem_session *s, const TotemHrtemArgs *h, Tot
 TOTEM_API int totem_hrtem_run(const TotemStemArgs *specimen, const TotemHrtemArgs *h, TotemHrtemOut *out);
 
 /* ---------------------------------------------------------------------------------------------
+ * Probe / image transfer functions (WholeTCC2D_newTEM, ToTEM_submit_v1.m:2305-2406), evaluated on
+ * the current device in FP64.  The reference computes them in MATLAB for every request.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct TotemAberrations {  /* magnitudes in nm, angles in degrees as entered in ToTem */
+  int struct_size;                 /* sizeof(TotemAberrations)                                 */
+  double focus;                    /* C1 */
+  double A1, phiA1, A2, phiA2, B2, phiB2;
+  double Cs;                       /* C3 */
+  double A3, phiA3, S3, phiS3, A4, phiA4, D4, phiD4, B4, phiB4, A5, phiA5;
+  double C5;
+  double S5, phiS5, D5, phiD5;
+} TotemAberrations;
+
+/* tcc[m][r][c] (centred grid, m = 0 .. steps-1) = E_s * E_f,m * exp(-i chi): chi from the
+ * aberrations to 5th order, the spatial envelope E_s of semi-angle alpha with the aberration
+ * gradient (with_gradient = 1, the reference's flag 2) or C1 alone, and focal-spread step m at
+ * (m + 1 - (steps + 1)/2) * delta_nm (Gaussian_focal gives delta and the weights).  lambda_nm is
+ * the electron wavelength; sampling_a the pixel size in Angstrom. */
+TOTEM_API int totem_tcc_stack(const TotemAberrations *ab, double lambda_nm, int n, double sampling_a,
+                              double alpha_mrad, int with_gradient, int steps, double delta_nm, double *tcc_re,
+                              double *tcc_im);
+
+/* ---------------------------------------------------------------------------------------------
  * Serving: a resident scheduler with continuous batching.  No counterpart in the reference,
  * whose entry point runs one blocking request at a time and allocates / frees everything per
  * call (waveCuda.cpp:4-101, cuda_source_lobato.cu:1018-1562).

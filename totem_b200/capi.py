@@ -93,6 +93,12 @@ class TotemServerStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TotemAberrations(C.Structure):
+    _fields_ = [("struct_size", C.c_int)] + [(f, C.c_double) for f in (
+        "focus", "A1", "phiA1", "A2", "phiA2", "B2", "phiB2", "Cs", "A3", "phiA3", "S3", "phiS3", "A4", "phiA4",
+        "D4", "phiD4", "B4", "phiB4", "A5", "phiA5", "C5", "S5", "phiS5", "D5", "phiD5")]
+
+
 class TotemError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"totem_b200 error {code}: {msg}")
@@ -140,6 +146,8 @@ def load() -> C.CDLL:
     lib.totem_server_info.argtypes = [vp, ull, C.POINTER(TotemRequestInfo)]
     lib.totem_server_destroy.argtypes = [vp]
     lib.totem_server_stats.argtypes = [vp, C.POINTER(TotemServerStats)]
+    lib.totem_tcc_stack.argtypes = [C.POINTER(TotemAberrations), C.c_double, C.c_int, C.c_double, C.c_double,
+                                    C.c_int, C.c_int, C.c_double, _dp, _dp]
     lib.totem_plan_simulate.argtypes = [C.c_int, _ip, C.POINTER(C.c_longlong), _ip, _ip, ull, ull, C.c_int, _ip, _ip,
                                         ullp]
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
@@ -147,7 +155,7 @@ def load() -> C.CDLL:
                  "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_session_hrtem",
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
-                 "totem_server_stats", "totem_plan_simulate"):
+                 "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -427,6 +435,22 @@ def _hrtem_marshal(spec, ph, pw, t_storage, exit_wave, image):
     def ex():
         return None if ere is None else ere + 1j * eim
     return h, out, ex, img
+
+
+def tcc_stack(ab, lambda_nm: float, n: int, sampling_a: float, alpha_mrad: float, with_gradient: bool, steps: int,
+              delta_nm: float) -> np.ndarray:
+    """``totem_tcc_stack``: the transfer functions (steps, n, n) complex128 on the centred grid,
+    evaluated on the device in FP64.  ``ab`` is an ``optics.Aberrations``."""
+    lib = load()
+    a = TotemAberrations()
+    a.struct_size = C.sizeof(TotemAberrations)
+    for name, _ in TotemAberrations._fields_[1:]:
+        setattr(a, name, float(getattr(ab, name)))
+    re_ = np.zeros((steps, n, n))
+    im_ = np.zeros((steps, n, n))
+    check(lib.totem_tcc_stack(C.byref(a), lambda_nm, n, sampling_a, alpha_mrad, int(with_gradient), steps, delta_nm,
+                              _ptr(re_), _ptr(im_)))
+    return re_ + 1j * im_
 
 
 def hrtem_run(specimen, spec, t_storage: int = T_COMPLEX64, exit_wave: bool = True, image: bool = True):

@@ -299,20 +299,26 @@ class ProbeSpec:
     focal_steps: int = 1               # mtotal
 
 
-def tcc_stack(spec: ProbeSpec, n: int, sampling_a: float, with_gradient: bool = True):
+def tcc_stack(spec: ProbeSpec, n: int, sampling_a: float, with_gradient: bool = True, engine: bool = False):
     """Per-defocus transfer functions (WholeTCC2D_newTEM, ToTEM_submit_v1.m:2305-2406).
 
     ``with_gradient`` selects the spatial envelope with the full aberration gradient
-    (the reference forces ``flag = 2`` at :2333 for both STEM and HRTEM).
+    (the reference forces ``flag = 2`` at :2333 for both STEM and HRTEM).  ``engine`` evaluates
+    the stack on the GPU (``totem_tcc_stack``, FP64) instead of in NumPy.
     Returns ``(tcc[m, n, n], gfsf[m])`` on the centred grid.
     """
     lam = wavelength_nm(spec.kv)
     samp_nm = sampling_a * 0.1
+    gmax = spec.semi_angle_mrad * 0.1  # tccpara.gmax (ToTEM_submit_v1.m:2166)
+    delta, gfsf = gaussian_focal_weights(spec.focal_steps, spec.focal_spread_nm, lam, gmax)
+    if engine:
+        from . import capi
+        tcc = capi.tcc_stack(spec.aberrations, lam, n, sampling_a, spec.convergence_mrad, with_gradient,
+                             spec.focal_steps, delta)
+        return tcc, np.asarray(gfsf, dtype=np.float64)
     half = int(math.floor((n + 1) / 2 + 0.5))  # MATLAB round((n+1)/2)
     ax = np.arange(-half + 1, n - half + 1, dtype=np.float64) / (samp_nm * n)
     U, V = np.meshgrid(ax, ax)
-    gmax = spec.semi_angle_mrad * 0.1  # tccpara.gmax (ToTEM_submit_v1.m:2166)
-    delta, gfsf = gaussian_focal_weights(spec.focal_steps, spec.focal_spread_nm, lam, gmax)
     ab = spec.aberrations
     A1x, A1y = ab.xy("A1")
     wu, wv = U * lam, V * lam
@@ -348,14 +354,14 @@ def aperture_mask(n: int, sampling_nm: float, k_outer: float) -> np.ndarray:
     return m
 
 
-def stem_probes(spec: ProbeSpec, n: int, sampling_a: float):
+def stem_probes(spec: ProbeSpec, n: int, sampling_a: float, engine: bool = False):
     """Normalised STEM probes, one per focal-spread step (ToTEM_submit_v1.m:800-818).
 
     Returns ``(probe[m, n, n] complex128, gfsf[m])``; each probe is centred (fftshift-ed) and
-    has unit L2 norm.
+    has unit L2 norm.  ``engine``: transfer functions on the GPU (``tcc_stack``).
     """
     lam = wavelength_nm(spec.kv)
-    tcc, gfsf = tcc_stack(spec, n, sampling_a, with_gradient=True)
+    tcc, gfsf = tcc_stack(spec, n, sampling_a, with_gradient=True, engine=engine)
     ap = aperture_mask(n, sampling_a * 0.1, spec.semi_angle_mrad * 0.1 * 0.01 / lam)
     probes = []
     for t in tcc:

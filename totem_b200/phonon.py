@@ -66,11 +66,12 @@ def main(argv=None):
                     help="probes of one configuration timed through the per-probe cuFFT path (0 = skip)")
     ns = ap.parse_args(argv)
 
-    def builder(phonon_seed):
+    def builder(phonon_seed, first=None):
         return request.build_srtio3_stem(cells=tuple(ns.cells), n=ns.window, raster=(ns.raster, ns.raster),
-                                         phonon_seed=phonon_seed)
+                                         phonon_seed=phonon_seed, engine_optics=True, optics_from=first)
     t0 = time.perf_counter()
-    configs = [builder(s) for s in range(ns.configs)]
+    configs = [builder(0)]
+    configs += [builder(s, configs[0]) for s in range(1, ns.configs)]
     t_build = time.perf_counter() - t0
     ps = sum(c.probe_slices for c in configs)
     frozen_phonon(configs[:1])  # warm-up
