@@ -21,6 +21,8 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <stdexcept>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -129,6 +131,7 @@ struct totem_server {
   void done_loop();
   Status prepare(Request* r);
   Status tick_once(totem::Planner& planner, int tick, bool* progressed);
+  Status lookup(unsigned long long ticket, Request** r);
   Status complete_request(Request* r);
   void fail_request(Request* r, const Status& s);
   void fail_all(const Status& s);
@@ -281,6 +284,16 @@ Status totem_server::complete_request(Request* r) {
   return Status::Ok();
 }
 
+// The running request of a probe group (every group's request stays in ``running`` until its last
+// group finished; a miss is an internal error, reported rather than thrown).
+Status totem_server::lookup(unsigned long long ticket, Request** r) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = running.find(ticket);
+  if (it == running.end()) return Status::Err(TOTEM_ERR_STATE, "scheduler: probe group of an unknown request");
+  *r = it->second;
+  return Status::Ok();
+}
+
 Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progressed) {
   *progressed = false;
   const int slot = tick % K;
@@ -292,10 +305,7 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
   std::vector<totem::PlanGroup> started = planner.start(tick);
   for (const totem::PlanGroup& g : started) {
     Request* r = nullptr;
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      r = running.at(g.req);
-    }
+    TOTEM_TRY(lookup(g.req, &r));
     void* psi = nullptr;
     void* part = nullptr;
     TOTEM_CUDA(cudaMallocFromPoolAsync(&psi, (size_t)g.items * g.n * g.n * sizeof(float2), pool, sst));
@@ -331,11 +341,8 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
     long long items = 0;
     for (size_t i = 0; i < ng; ++i) {
       const totem::PlanGroup& g = *gs[i];
-      Request* r;
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        r = running.at(g.req);
-      }
+      Request* r = nullptr;
+      TOTEM_TRY(lookup(g.req, &r));
       const totem_session* s = r->sess;
       totem::GroupDesc& x = desc[i];
       x.psi = static_cast<float2*>(g.psi);
@@ -367,11 +374,8 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
   }
   // groups that ran their last slice: detector sums, then their wave memory goes back
   for (const totem::PlanGroup& g : planner.finish(tick)) {
-    Request* r;
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      r = running.at(g.req);
-    }
+    Request* r = nullptr;
+    TOTEM_TRY(lookup(g.req, &r));
     const totem_session* s = r->sess;
     const long ad = (long)s->aper_num * s->depth;
     const size_t estride = (size_t)g.items * s->aper_num * r->nblk;
@@ -530,6 +534,22 @@ void shutdown(totem_server* s) {
 
 }  // namespace
 
+// Worker thread body.  A host exception (allocation failure) fails every pending request instead
+// of terminating the caller's process; the worker then exits as on shutdown.
+void run_worker(totem_server* s, int which) {
+  try {
+    if (which == 0) s->prep_loop();
+    else if (which == 1) s->sched_loop();
+    else s->done_loop();
+  } catch (const std::exception& e) {
+    s->fail_all(Status::Err(TOTEM_ERR_OOM, std::string("server worker: ") + e.what()));
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (which == 0) s->prep_exited = true;
+    if (which == 1) s->sched_exited = true;
+    s->cv.notify_all();
+  }
+}
+
 extern "C" {
 
 int totem_server_create(const TotemServerOptions* opt, totem_server** out) {
@@ -557,9 +577,9 @@ int totem_server_create(const TotemServerOptions* opt, totem_server** out) {
     return server_fail(st);
   }
   totem_server* raw = s.get();
-  raw->prep_thr = std::thread([raw] { raw->prep_loop(); });
-  raw->sched_thr = std::thread([raw] { raw->sched_loop(); });
-  raw->done_thr = std::thread([raw] { raw->done_loop(); });
+  raw->prep_thr = std::thread(run_worker, raw, 0);
+  raw->sched_thr = std::thread(run_worker, raw, 1);
+  raw->done_thr = std::thread(run_worker, raw, 2);
   *out = s.release();
   return TOTEM_OK;
 }
