@@ -297,6 +297,8 @@ typedef struct TotemServerOptions {
   unsigned long long chunk_bytes;/* wave bytes one request may claim per tick; 0 = wave_bytes/4 */
   int ticks_ahead;               /* slice steps queued ahead of the GPU; 0 = 4                 */
   int policy;                    /* TOTEM_SCHED_*                                              */
+  int prep_threads;              /* host threads preparing requests (upload, transmission);
+                                    0 = 1                                                      */
 } TotemServerOptions;
 
 enum {

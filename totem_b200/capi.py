@@ -76,7 +76,7 @@ class TotemTiming(C.Structure):
 class TotemServerOptions(C.Structure):
     _fields_ = [("struct_size", C.c_int), ("device", C.c_int), ("hbm_budget", C.c_ulonglong),
                 ("wave_bytes", C.c_ulonglong), ("chunk_bytes", C.c_ulonglong), ("ticks_ahead", C.c_int),
-                ("policy", C.c_int)]
+                ("policy", C.c_int), ("prep_threads", C.c_int)]
 
 
 class TotemRequestInfo(C.Structure):
@@ -331,10 +331,10 @@ class Server:
     """
 
     def __init__(self, device: int = -1, hbm_budget: int = 0, wave_bytes: int = 0, chunk_bytes: int = 0,
-                 ticks_ahead: int = 0, policy: int = SCHED_SHORTEST):
+                 ticks_ahead: int = 0, policy: int = SCHED_SHORTEST, prep_threads: int = 0):
         self.lib = load()
         o = TotemServerOptions(C.sizeof(TotemServerOptions), device, hbm_budget, wave_bytes, chunk_bytes,
-                               ticks_ahead, policy)
+                               ticks_ahead, policy, prep_threads)
         h = C.c_void_p()
         check(self.lib.totem_server_create(C.byref(o), C.byref(h)))
         self.h = h

@@ -18,6 +18,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "session.h"
@@ -83,22 +84,33 @@ totem::SpeciesHost group_species(const RowsHost& h, int slices) {
   sp.seg_beg.assign(slices + 1, 0);
   sp.pos.reserve(h.pos.size());
   const bool ab = !h.absorp.empty();
-  std::map<std::vector<float>, int> ids;
-  std::vector<float> key;
+  // key: the bytes of the coefficient row (and absorptive row); rows of one species usually come
+  // in runs, so the previous row's id is tried first
+  std::unordered_map<std::string, int> ids;
+  std::string key, prev_key;
+  int prev_id = -1;
+  const size_t cbytes = (size_t)h.ncoef * sizeof(float);
   for (int s = 0; s < slices && h.count > 0; ++s) {
     std::vector<int> order;              // species in order of appearance in this slice
     std::map<int, std::vector<int>> atoms;
     for (int a = h.beg[s]; a < h.beg[s + 1]; ++a) {
-      key.assign(h.coef.begin() + (size_t)a * h.ncoef, h.coef.begin() + (size_t)(a + 1) * h.ncoef);
-      if (ab) key.insert(key.end(), h.absorp.begin() + (size_t)a * 10, h.absorp.begin() + (size_t)(a + 1) * 10);
-      auto it = ids.find(key);
-      if (it == ids.end()) {
-        it = ids.emplace(key, (int)ids.size()).first;
-        sp.coef.insert(sp.coef.end(), key.begin(), key.begin() + h.ncoef);
-        if (ab) sp.absorp.insert(sp.absorp.end(), key.begin() + h.ncoef, key.end());
+      key.assign(reinterpret_cast<const char*>(h.coef.data() + (size_t)a * h.ncoef), cbytes);
+      if (ab) key.append(reinterpret_cast<const char*>(h.absorp.data() + (size_t)a * 10), 10 * sizeof(float));
+      int id = prev_id;
+      if (prev_id < 0 || key != prev_key) {
+        auto it = ids.find(key);
+        if (it == ids.end()) {
+          it = ids.emplace(key, (int)ids.size()).first;
+          const float* f = reinterpret_cast<const float*>(key.data());
+          sp.coef.insert(sp.coef.end(), f, f + h.ncoef);
+          if (ab) sp.absorp.insert(sp.absorp.end(), f + h.ncoef, f + h.ncoef + 10);
+        }
+        id = it->second;
+        prev_key = key;
+        prev_id = id;
       }
-      auto& v = atoms[it->second];
-      if (v.empty()) order.push_back(it->second);
+      auto& v = atoms[id];
+      if (v.empty()) order.push_back(id);
       v.push_back(a);
     }
     for (int id : order) {

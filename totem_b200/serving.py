@@ -95,7 +95,11 @@ def serve(reqs, arrivals, policy: int = capi.SCHED_SHORTEST, **server_kw):
             tickets.append(srv.submit(req))
         results = [srv.wait(t) for t in tickets]
         makespan = time.perf_counter() - t0
-        lat = np.array([srv.info(t).latency_ms for t in tickets])
+        infos = [srv.info(t) for t in tickets]
+        lat = np.array([i.latency_ms for i in infos])
+        serve.last_phases = {k: float(np.mean([getattr(i, k) for i in infos]))
+                             for k in ("queued_ms", "prepare_ms", "run_ms")}
+        serve.last_stats = srv.stats()
     return results, lat, makespan
 
 
@@ -133,22 +137,26 @@ def main(argv=None):
     ap.add_argument("--load", type=float, default=0.85, help="offered load as a fraction of burst capacity")
     ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
     ap.add_argument("--wave-mib", type=int, default=0, help="wave memory of the server (0 = its default)")
+    ap.add_argument("--prep-threads", type=int, default=0, help="server preparation threads (0 = its default)")
     ap.add_argument("--compare", action="store_true", help="also serve one request at a time")
     ns = ap.parse_args(argv)
     policy = capi.SCHED_SHORTEST if ns.policy == "shortest" else capi.SCHED_FIFO
     reqs = make_workload(ns.requests, ns.seed, tuple(ns.sizes), ns.max_probes, tuple(ns.slices))
     kw = {"wave_bytes": ns.wave_mib << 20} if ns.wave_mib else {}
+    if ns.prep_threads:
+        kw["prep_threads"] = ns.prep_threads
     # warm-up (kernels, pools) on a few requests, then the burst capacity
     serve(reqs[:4], np.zeros(4), policy, **kw)
     res_b, lat_b, mk_b = serve(reqs, np.zeros(len(reqs)), policy, **kw)
-    out = [summary("burst", reqs, lat_b, mk_b)]
+    out = [dict(summary("burst", reqs, lat_b, mk_b), phases_mean=serve.last_phases, server=serve.last_stats)]
     if ns.compare:
         _, lat_sb, mk_sb = serve_one_at_a_time(reqs, np.zeros(len(reqs)))
         out.append(summary("one-at-a-time burst", reqs, lat_sb, mk_sb))
     rate = ns.rate or ns.load * len(reqs) / mk_b
     arr = poisson_arrivals(len(reqs), rate, ns.seed)
     res_p, lat_p, mk_p = serve(reqs, arr, policy, **kw)
-    out.append(dict(summary("poisson", reqs, lat_p, mk_p), rate_hz=rate))
+    out.append(dict(summary("poisson", reqs, lat_p, mk_p), rate_hz=rate, phases_mean=serve.last_phases,
+                    server=serve.last_stats))
     if ns.compare:
         res_s, lat_s, mk_s = serve_one_at_a_time(reqs, arr)
         out.append(dict(summary("one-at-a-time", reqs, lat_s, mk_s), rate_hz=rate))
