@@ -60,6 +60,23 @@ struct Request {
   size_t item_bytes = 0;
   long long probe_slices = 0;
   double est = 0;                   // estimated device seconds (preparation order)
+  int lane = 1;                     // 0 fast, 1 bulk
+};
+
+// A tick loop: its own planner, tick counter, stream and staging ring.  Lane 0 (fast) takes the
+// requests whose probe waves fit it whole and runs on the highest stream priority, so a small
+// request advances one slice per short tick instead of one slice per tick of the large requests
+// beside it; lane 1 (bulk) takes the rest.  Both lanes' launches run concurrently on the device.
+struct Lane {
+  totem::Planner planner;
+  cudaStream_t st = nullptr;
+  int tick = 0;
+  char* h_stage = nullptr;          // pinned [K][slot_bytes]
+  char* d_stage = nullptr;          // device [K][slot_bytes]
+  std::vector<cudaEvent_t> tick_ev;
+  size_t wave = 0;
+  Lane(size_t wave_bytes, size_t chunk, int policy, size_t max_groups)
+      : planner(wave_bytes, chunk, policy, max_groups), wave(wave_bytes) {}
 };
 
 // Resident bytes of a request outside its probe waves (upper estimate, pool slack included).
@@ -101,7 +118,7 @@ struct totem_server {
   int device = 0;
   TotemServerOptions opt{};
   cudaMemPool_t pool = nullptr;
-  cudaStream_t sst = nullptr;
+  std::vector<std::unique_ptr<Lane>> lanes;
   size_t static_budget = 0, static_used = 0;
 
   std::mutex mu;
@@ -121,9 +138,6 @@ struct totem_server {
   std::map<int, std::unique_ptr<totem::DevBuf>> tw;  // stage twiddles per window size
   int K = 4;                                         // ticks queued ahead
   size_t slot_bytes = 0;
-  char* h_stage = nullptr;                           // pinned [K][slot_bytes]
-  char* d_stage = nullptr;                           // device [K][slot_bytes]
-  std::vector<cudaEvent_t> tick_ev;
   size_t max_groups = 4096;
   TotemServerStats stats{};  // guarded by mu
 
@@ -132,7 +146,7 @@ struct totem_server {
   void sched_loop();
   void done_loop();
   Status prepare(Request* r);
-  Status tick_once(totem::Planner& planner, int tick, bool* progressed);
+  Status tick_once(Lane& lane, bool* progressed);
   Status lookup(unsigned long long ticket, Request** r);
   Status complete_request(Request* r);
   void fail_request(Request* r, const Status& s);
@@ -148,11 +162,6 @@ Status totem_server::init() {
   TOTEM_CUDA(cudaMemPoolCreate(&pool, &props));
   unsigned long long keep = ~0ull;  // keep freed memory in the pool for the next request
   TOTEM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-  // The tick stream runs at the highest priority, so slice steps of running requests are not
-  // queued behind the transmission builds of requests being prepared (default priority).
-  int least = 0, greatest = 0;
-  TOTEM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-  TOTEM_CUDA(cudaStreamCreateWithPriority(&sst, cudaStreamNonBlocking, greatest));
   size_t fr = 0, tot = 0;
   TOTEM_CUDA(cudaMemGetInfo(&fr, &tot));
   size_t budget = opt.hbm_budget ? (size_t)opt.hbm_budget : (size_t)(0.9 * (double)fr);
@@ -164,12 +173,25 @@ Status totem_server::init() {
   static_budget = budget - wave;
   K = opt.ticks_ahead > 0 ? opt.ticks_ahead : 4;
   slot_bytes = max_groups * (sizeof(totem::GroupDesc) + sizeof(int)) + 64 * (sizeof(int) + 256);
-  TOTEM_CUDA(cudaMallocHost(&h_stage, slot_bytes * K));
-  TOTEM_CUDA(cudaMalloc(&d_stage, slot_bytes * K));
-  tick_ev.assign(K, nullptr);
-  // blocking-sync events: a thread waiting for the device sleeps instead of spinning on a core
-  // that the preparation threads need
-  for (auto& e : tick_ev) TOTEM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync));
+  // Tick streams run above the default priority of the preparation streams, so slice steps of
+  // running requests are not queued behind transmission builds; the fast lane above the bulk lane.
+  int least = 0, greatest = 0;
+  TOTEM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  const size_t fast_wave = std::min<size_t>(256ull << 20, wave / 4);
+  for (int l = 0; l < 2; ++l) {
+    const size_t w = l == 0 ? fast_wave : wave;
+    lanes.emplace_back(new Lane(w, l == 0 ? w : opt.chunk_bytes, opt.policy, max_groups));
+    Lane& ln = *lanes.back();
+    const int prio = l == 0 ? greatest : std::min(least, greatest + 1);
+    TOTEM_CUDA(cudaStreamCreateWithPriority(&ln.st, cudaStreamNonBlocking, prio));
+    TOTEM_CUDA(cudaMallocHost(&ln.h_stage, slot_bytes * K));
+    TOTEM_CUDA(cudaMalloc(&ln.d_stage, slot_bytes * K));
+    ln.tick_ev.assign(K, nullptr);
+    // blocking-sync events: a thread waiting for the device sleeps instead of spinning on a core
+    // that the preparation thread needs
+    for (auto& e : ln.tick_ev)
+      TOTEM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync));
+  }
   return Status::Ok();
 }
 
@@ -274,7 +296,7 @@ void totem_server::prep_loop() {
 // ---------------------------------------------------------------------------------------------
 Status totem_server::complete_request(Request* r) {
   totem_session* s = r->sess;
-  TOTEM_CUDA(cudaEventRecord(r->handoff, sst));
+  TOTEM_CUDA(cudaEventRecord(r->handoff, lanes[r->lane]->st));
   TOTEM_CUDA(cudaStreamWaitEvent(s->stream, r->handoff, 0));
   int launches = 0;
   if (r->items > 0) TOTEM_TRY(s->combine_results(r->de, &launches));
@@ -298,11 +320,14 @@ Status totem_server::lookup(unsigned long long ticket, Request** r) {
   return Status::Ok();
 }
 
-Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progressed) {
+Status totem_server::tick_once(Lane& lane, bool* progressed) {
   *progressed = false;
+  totem::Planner& planner = lane.planner;
+  const int tick = lane.tick;
+  cudaStream_t sst = lane.st;
   const int slot = tick % K;
   const Clock::time_point t0 = Clock::now();
-  TOTEM_CUDA(cudaEventSynchronize(tick_ev[slot]));  // tick - K has finished: its staging slot is free
+  TOTEM_CUDA(cudaEventSynchronize(lane.tick_ev[slot]));  // tick - K has finished: its slot is free
   const Clock::time_point t1 = Clock::now();
   long long launched = 0, advanced = 0;
   // start the admitted groups
@@ -324,8 +349,8 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
   // one row and one column launch per window size over every active group
   std::map<int, std::vector<const totem::PlanGroup*>> by_n;
   for (const totem::PlanGroup& g : act) by_n[g.n].push_back(&g);
-  char* h = h_stage + (size_t)slot * slot_bytes;
-  char* d = d_stage + (size_t)slot * slot_bytes;
+  char* h = lane.h_stage + (size_t)slot * slot_bytes;
+  char* d = lane.d_stage + (size_t)slot * slot_bytes;
   size_t off = 0;
   for (auto& kv : by_n) {
     const int n = kv.first;
@@ -334,6 +359,7 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
     if (!twb) {
       twb.reset(new totem::DevBuf());
       TOTEM_TRY(totem::upload(*twb, totem::twiddles(n), sst));
+      TOTEM_CUDA(cudaStreamSynchronize(sst));  // once per window size: the other lane may use it next
     }
     const size_t ng = gs.size();
     const size_t desc_off = off, ib_off = off + ng * sizeof(totem::GroupDesc);
@@ -393,7 +419,7 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
     r->items_left -= g.items;
     if (r->items_left == 0) TOTEM_TRY(complete_request(r));
   }
-  TOTEM_CUDA(cudaEventRecord(tick_ev[slot], sst));
+  TOTEM_CUDA(cudaEventRecord(lane.tick_ev[slot], sst));
   std::lock_guard<std::mutex> lk(mu);
   stats.ticks += 1;
   stats.probe_slices += advanced;
@@ -406,17 +432,16 @@ Status totem_server::tick_once(totem::Planner& planner, int tick, bool* progress
 
 void totem_server::sched_loop() {
   cudaSetDevice(device);
-  totem::Planner planner(opt.wave_bytes, opt.chunk_bytes, opt.policy, max_groups);
-  int tick = 0;
+  auto idle = [&] { return lanes[0]->planner.idle() && lanes[1]->planner.idle(); };
   for (;;) {
     std::vector<Request*> fresh;
     {
       std::unique_lock<std::mutex> lk(mu);
       const Clock::time_point w0 = Clock::now();
-      cv.wait(lk, [&] { return !ready.empty() || !planner.idle() || (stopping && prep_exited) || !fatal.ok(); });
+      cv.wait(lk, [&] { return !ready.empty() || !idle() || (stopping && prep_exited) || !fatal.ok(); });
       stats.idle_ms += ms_between(w0, Clock::now());
       if (!fatal.ok()) break;
-      if (ready.empty() && planner.idle() && stopping && prep_exited) break;
+      if (ready.empty() && idle() && stopping && prep_exited) break;
       while (!ready.empty()) {
         fresh.push_back(ready.front());
         ready.pop_front();
@@ -429,7 +454,8 @@ void totem_server::sched_loop() {
     }
     Status st;
     for (Request* r : fresh) {
-      st = totem::cuda_status(cudaStreamWaitEvent(sst, r->ready, 0), "cudaStreamWaitEvent");
+      r->lane = (r->items * r->item_bytes <= lanes[0]->wave) ? 0 : 1;
+      st = totem::cuda_status(cudaStreamWaitEvent(lanes[r->lane]->st, r->ready, 0), "cudaStreamWaitEvent");
       if (!st.ok()) break;
       if (r->items == 0) {
         st = complete_request(r);
@@ -442,19 +468,20 @@ void totem_server::sched_loop() {
       pr.items = r->items;
       pr.slices = r->sess->slices;
       pr.item_bytes = r->item_bytes;
-      planner.add(pr);
+      lanes[r->lane]->planner.add(pr);
     }
-    bool progressed = false;
-    if (st.ok() && !planner.idle()) {
-      st = tick_once(planner, tick, &progressed);
-      if (progressed) ++tick;
+    for (auto& lane : lanes) {
+      if (!st.ok() || lane->planner.idle()) continue;
+      bool progressed = false;
+      st = tick_once(*lane, &progressed);
+      if (progressed) ++lane->tick;
     }
     if (!st.ok()) {
       fail_all(st);
       break;
     }
   }
-  cudaStreamSynchronize(sst);
+  for (auto& lane : lanes) cudaStreamSynchronize(lane->st);
   std::lock_guard<std::mutex> lk(mu);
   sched_exited = true;
   cv.notify_all();
@@ -525,12 +552,15 @@ void shutdown(totem_server* s) {
       kv.second->sess = nullptr;
     }
   s->tw.clear();
-  if (s->sst) cudaStreamSynchronize(s->sst);
-  for (auto& e : s->tick_ev)
-    if (e) cudaEventDestroy(e);
-  if (s->h_stage) cudaFreeHost(s->h_stage);
-  if (s->d_stage) cudaFree(s->d_stage);
-  if (s->sst) cudaStreamDestroy(s->sst);
+  for (auto& lane : s->lanes) {
+    if (lane->st) cudaStreamSynchronize(lane->st);
+    for (auto& e : lane->tick_ev)
+      if (e) cudaEventDestroy(e);
+    if (lane->h_stage) cudaFreeHost(lane->h_stage);
+    if (lane->d_stage) cudaFree(lane->d_stage);
+    if (lane->st) cudaStreamDestroy(lane->st);
+  }
+  s->lanes.clear();
   if (s->pool) {
     cudaDeviceSynchronize();
     cudaMemPoolDestroy(s->pool);
