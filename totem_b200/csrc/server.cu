@@ -192,6 +192,14 @@ Status totem_server::init() {
     for (auto& e : ln.tick_ev)
       TOTEM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync));
   }
+  // Map the pool's memory once up front (the waves plus a few transmission stacks): growing a
+  // pool maps new physical memory, which took tens of milliseconds per request when request
+  // sizes grew; freed memory stays in the pool (release threshold) for suballocation.
+  const size_t reserve = std::min<size_t>(budget, wave + (4ull << 30));
+  void* warm = nullptr;
+  TOTEM_CUDA(cudaMallocFromPoolAsync(&warm, reserve, pool, lanes[1]->st));
+  TOTEM_CUDA(cudaFreeAsync(warm, lanes[1]->st));
+  TOTEM_CUDA(cudaStreamSynchronize(lanes[1]->st));
   return Status::Ok();
 }
 
