@@ -233,6 +233,9 @@ def main():
 
     import torch
     ws, rank, local = dist_env()
+    # the one-shot C ABI (the e2e leg) picks its device by free memory unless TOTEM_DEVICE is set:
+    # pin it to this rank's GPU
+    os.environ["TOTEM_DEVICE"] = str(local)
     dist = None
     if ws > 1:
         import datetime
