@@ -171,6 +171,29 @@ TOTEM_API int totem_stem_run(const TotemStemArgs *args, const TotemRunOptions *o
  * transmission exp(i sigma V / 1000)).  Replaces cuda_source_lobato_potential.cu:747. */
 TOTEM_API int totem_transmission_run(const TotemStemArgs *args, TotemStemOut *out);
 
+/* How the neutral and ionic potential sums are formed on separable reciprocal grids (the
+ * reference's meshgrid layout).  Process-wide; later transmission builds use it.  No
+ * counterpart in the reference, whose cal_p sums every atom at every pixel.
+ *   TOTEM_TX_AUTO      the cheaper of the two by a cost model (default)
+ *   TOTEM_TX_DIRECT    per-species sums over atoms at every pixel: O(atoms x pixels)
+ *   TOTEM_TX_GRIDDING  Gaussian gridding onto a twice-finer grid and FFTs (a non-uniform FFT):
+ *                      O(atoms + pixels log pixels), relative error ~1e-7; used where the axes
+ *                      are uniform and the grid is a power of two from 64 to 4096, otherwise
+ *                      DIRECT is used.
+ * ``scratch_bytes`` bounds the gridding work memory taken during a build (0 = 1 GiB); at least
+ * one species plane set (64 bytes per potential pixel) is always taken. */
+#define TOTEM_TX_AUTO 0
+#define TOTEM_TX_DIRECT 1
+#define TOTEM_TX_GRIDDING 2
+TOTEM_API int totem_set_tx_builder(int mode, size_t scratch_bytes);
+/* The gridding builder's batch plan, without a device (tests): jobs are numbered in slice order,
+ * slice s owning jobs [job_beg[s], job_beg[s+1]); at most jobs_per_batch jobs run per batch.
+ * Writes up to max_batches rows (s_lo, s_hi, j_lo, j_hi) to ``out`` and the batch count to
+ * ``count``: batch b runs jobs [j_lo, j_hi) and writes slices [s_lo, s_hi), adding to a slice
+ * whose first job ran in an earlier batch. */
+TOTEM_API int totem_grid_batches(const int *job_beg, int slices, int jobs_per_batch, int *out, int max_batches,
+                                 int *count);
+
 /* Size of the fixed device scratch array used by totem_stem_slices_noalloc (per GPU). */
 #define TOTEM_NOALLOC_SCRATCH_BYTES (32ull << 20)
 

@@ -100,3 +100,10 @@ def test_null_arguments_are_rejected(lib):
     assert lib.totem_session_upload(None, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_run(None, 0, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_destroy(None) == capi.OK
+
+
+def test_builder_choice_is_validated(lib):
+    # a process-wide setting: no device needed
+    assert lib.totem_set_tx_builder(7, 0) == capi.ERR_INVALID_ARG
+    assert lib.totem_set_tx_builder(capi.TX_GRIDDING, 1 << 20) == capi.OK
+    assert lib.totem_set_tx_builder(capi.TX_AUTO, 0) == capi.OK

@@ -80,31 +80,10 @@ def test_defocus_spread_and_unsorted_layers(engine_lib):
 
 
 def test_absorptive_and_ionic_rows(engine_lib):
-    from totem_b200 import specimen
-    req = request.build_small_stem(flag="p")
-    # turn a third of the atoms into partly ionic O (O2-), plus absorptive rows on everything
-    rows = req.ele_n
-    n = len(rows)
-    ion_idx = np.arange(0, n, 3)
-    o2 = specimen.ion_params(8, -2)
-    neutral_o = specimen.element_params(8, "p")
-    ion_rows = np.zeros((len(ion_idx), 25))
-    ion_rows[:, 0:3] = rows[ion_idx, 0:3]
-    ion_rows[:, 3] = 0.4
-    ion_rows[:, 4:14:2], ion_rows[:, 5:14:2] = o2[:5], o2[5:]
-    ion_rows[:, 14] = 0.6
-    ion_rows[:, 15:25:2], ion_rows[:, 16:25:2] = neutral_o[:5], neutral_o[5:]
-    keep = np.setdiff1d(np.arange(n), ion_idx)
-    # per-slice counts of both kinds
-    beg = np.concatenate([[0], np.cumsum(req.series_n)]).astype(int)
-    sl = np.searchsorted(beg, np.arange(n), side="right") - 1
-    series_n = np.bincount(sl[keep], minlength=req.slices).astype(float)
-    series_i = np.bincount(sl[ion_idx], minlength=req.slices).astype(float)
-    from dataclasses import replace
-    req2 = replace(req, ele_n=rows[keep], series_n=series_n, ele_n_i=ion_rows, series_n_i=series_i)
-    req2 = request.with_absorption(req2)
-    res, mid = capi.stem_run(req2)
-    _check(req2, res, mid)
+    # a third of the atoms as partly ionic O (O2-), plus absorptive rows on everything
+    req = request.with_absorption(request.with_ionic_oxygen(request.build_small_stem(flag="p")))
+    res, mid = capi.stem_run(req)
+    _check(req, res, mid)
 
 
 def test_session_reuse_and_batches(engine_lib):

@@ -4,6 +4,7 @@ Loading fails loudly when the shared library is missing: there is no CPU or PyTo
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import re
@@ -148,6 +149,8 @@ def load() -> C.CDLL:
     lib.totem_server_stats.argtypes = [vp, C.POINTER(TotemServerStats)]
     lib.totem_tcc_stack.argtypes = [C.POINTER(TotemAberrations), C.c_double, C.c_int, C.c_double, C.c_double,
                                     C.c_int, C.c_int, C.c_double, _dp, _dp]
+    lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
+    lib.totem_grid_batches.argtypes = [_ip, C.c_int, C.c_int, _ip, C.c_int, _ip]
     lib.totem_plan_simulate.argtypes = [C.c_int, _ip, C.POINTER(C.c_longlong), _ip, _ip, ull, ull, C.c_int, _ip, _ip,
                                         ullp]
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
@@ -155,7 +158,8 @@ def load() -> C.CDLL:
                  "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_session_hrtem",
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
-                 "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack"):
+                 "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
+                 "totem_grid_batches"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -472,6 +476,40 @@ def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
     opt = TotemRunOptions(path, batch, 0, 0, 0, T_COMPLEX64)
     check(lib.totem_stem_run(C.byref(m.args), C.byref(opt), C.byref(out)))
     return res, mid
+
+
+TX_AUTO, TX_DIRECT, TX_GRIDDING = 0, 1, 2
+
+
+def set_tx_builder(mode: int, scratch_bytes: int = 0):
+    """Process-wide transmission builder for separable grids (``totem_set_tx_builder``):
+    TX_AUTO (cost model), TX_DIRECT (sums over atoms at every pixel) or TX_GRIDDING (Gaussian
+    gridding + FFT where the axes are uniform); ``scratch_bytes`` bounds the gridding work memory
+    (0 = the library default)."""
+    check(load().totem_set_tx_builder(int(mode), int(scratch_bytes)))
+
+
+def grid_batches(job_beg, jobs_per_batch: int) -> np.ndarray:
+    """The gridding builder's batch plan (``totem_grid_batches``): rows (s_lo, s_hi, j_lo, j_hi)."""
+    lib = load()
+    jb = np.ascontiguousarray(job_beg, dtype=np.int32)
+    slices = len(jb) - 1
+    cnt = C.c_int(0)
+    cap = 2 * (int(jb[-1]) + slices) + 2
+    out = np.zeros((cap, 4), dtype=np.int32)
+    check(lib.totem_grid_batches(jb.ctypes.data_as(_ip), slices, int(jobs_per_batch),
+                                 out.ctypes.data_as(_ip), cap, C.byref(cnt)))
+    return out[:cnt.value]
+
+
+@contextlib.contextmanager
+def tx_builder(mode: int, scratch_bytes: int = 0):
+    """``set_tx_builder`` for the duration of a ``with`` block, then back to TX_AUTO."""
+    set_tx_builder(mode, scratch_bytes)
+    try:
+        yield
+    finally:
+        set_tx_builder(TX_AUTO, 0)
 
 
 def transmission_run(req):

@@ -100,6 +100,35 @@ Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const At
 // and pixel.  Overwrites out.
 Status launch_tx_species(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, float2* out,
                          cudaStream_t st);
+// The same sums by Gaussian gridding (a type-1 non-uniform FFT) on uniform separable grids.
+// Work is grouped in jobs, one per (slice, kind, species) segment, ordered by slice; a batch
+// runs the jobs [j_lo, j_hi) in scratch memory and writes slices [s_lo, s_hi) (the last may be
+// partial, finished by the next batch).
+struct GridPlanDev {
+  double dkx = 0, dky = 0;         // spacing of the kx / ky axes
+  double sx = 0, sy = 0;           // kx(p_w / 2), ky(p_h / 2): the shift folded into each atom's weight
+  const float2* ax = nullptr;      // [p_w][2]: Gaussian deconvolution x half-bin phase (parity 0, 1)
+  const float2* ay = nullptr;      // [p_h][2]
+  const int4* jobs = nullptr;      // [jobs]: kind, species, first atom, end atom
+  const int* job_beg = nullptr;    // [slices + 1] first job of every slice
+};
+struct GridBatch {
+  int s_lo, s_hi, j_lo, j_hi;
+};
+std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_per_batch);
+// Scratch of one job: four p_h x p_w planes of 16-byte points.
+inline size_t grid_job_bytes(int p_h, int p_w) { return (size_t)p_h * p_w * 64; }
+// Overwrites out like launch_tx_species; ``scratch`` holds at least one job.
+Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, const GridPlanDev& gp,
+                          const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,
+                          const float2* tw_h, void* scratch, size_t scratch_bytes, float2* out, cudaStream_t st,
+                          int* launches);
+// Per-axis factors of the gridding builder for an axis of n points: [c][parity] = the inverse
+// of the spreading Gaussian's transform (normalised) times exp(-i pi k parity / n), k = c - n/2.
+std::vector<float2> grid_deconvolution(int n);
+// Process-wide builder choice for separable grids (TOTEM_TX_*) and gridding scratch bytes.
+int tx_builder_mode();
+size_t tx_gridding_scratch();
 // In-place unnormalised inverse 2-D FFT of every slice, times (-1)^(r+c) (the ifftshift of the
 // input), then T = exp(i * sigma_scaled * V).  Powers of two only; returns
 // TOTEM_ERR_UNSUPPORTED otherwise.

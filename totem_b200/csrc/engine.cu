@@ -10,6 +10,7 @@
 //    (cuda_source_lobato.cu:1250);
 //  * every CUDA / cuFFT status is checked and returned as a TOTEM_ERR_* code.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -34,6 +35,8 @@ using totem::g_h2d_bytes;
 namespace {
 
 thread_local std::string g_last_error;
+std::atomic<int> g_tx_mode{TOTEM_TX_AUTO};
+std::atomic<size_t> g_tx_scratch{0};
 
 int fail(const Status& s) {
   g_last_error = s.msg;
@@ -130,6 +133,12 @@ totem::SpeciesHost group_species(const RowsHost& h, int slices) {
 }  // namespace
 
 void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int totem::tx_builder_mode() { return g_tx_mode.load(); }
+size_t totem::tx_gridding_scratch() {
+  const size_t b = g_tx_scratch.load();
+  return b ? b : (1ull << 30);
+}
 
 thread_local long long totem::g_h2d_bytes = 0;
 
@@ -252,9 +261,12 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
         break;
       }
   // neutral / ionic rows: by species on separable grids (k_tx_species), row by row otherwise
+  grid_ok = false;
   if (separable) {
-    TOTEM_TRY(species_n.put(group_species(host_n, slices), st));
-    TOTEM_TRY(species_i.put(group_species(host_i, slices), st));
+    const totem::SpeciesHost spn = group_species(host_n, slices), spi = group_species(host_i, slices);
+    TOTEM_TRY(species_n.put(spn, st));
+    TOTEM_TRY(species_i.put(spi, st));
+    TOTEM_TRY(plan_gridding(a, spn, spi));
   } else {
     TOTEM_TRY(rows_n.put(host_n, st));
     TOTEM_TRY(rows_i.put(host_i, st));
@@ -339,8 +351,25 @@ Status totem_session::build_transmission(int path, int* launches) {
   if (separable) {
     const auto sn = species_n.view(n_rows > 0, has_abs_n, ncoef_n);
     const auto si = species_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
-    TOTEM_TRY(totem::launch_tx_species(g, sn, si, T.as<float2>(), stream));
-    ++*launches;
+    const int mode = totem::tx_builder_mode();
+    if (grid_ok && (mode == TOTEM_TX_GRIDDING || (mode == TOTEM_TX_AUTO && gridding_cheaper()))) {
+      const size_t job = totem::grid_job_bytes(p_h, p_w);
+      const size_t jobs = std::max<size_t>(grid_jobs_h.size(), 1);
+      const size_t bytes = std::max<size_t>(1, std::min(totem::tx_gridding_scratch() / job, jobs)) * job;
+      TOTEM_TRY(grid_scratch.ensure(bytes));
+      totem::GridPlanDev gp;
+      gp.dkx = grid_dkx; gp.dky = grid_dky; gp.sx = grid_sx; gp.sy = grid_sy;
+      gp.ax = grid_ax.as<float2>(); gp.ay = grid_ay.as<float2>();
+      gp.jobs = grid_jobs.as<int4>(); gp.job_beg = grid_job_beg.as<int>();
+      TOTEM_TRY(totem::launch_tx_gridding(g, sn, si, gp, grid_job_beg_h, grid_jobs_h, tw_pw.as<float2>(),
+                                          tw_ph.as<float2>(), grid_scratch.p, bytes, T.as<float2>(), stream, launches));
+      // work memory of the build only: returned at once to a server's pool (stream-ordered and
+      // cheap); a plain session keeps it for its next build (cudaFree would synchronise)
+      if (grid_scratch.pool) grid_scratch.release();
+    } else {
+      TOTEM_TRY(totem::launch_tx_species(g, sn, si, T.as<float2>(), stream));
+      ++*launches;
+    }
     if (vcn.beg || vci.beg) {  // Peng-extended correction rows: per-pixel maps, row by row
       TOTEM_TRY(totem::launch_tx_structure(g, totem::AtomRowsDev{}, totem::AtomRowsDev{}, vcn, vci, T.as<float2>(),
                                            stream, true));
@@ -367,6 +396,67 @@ Status totem_session::build_transmission(int path, int* launches) {
   t_valid = true;
   tb_valid = false;
   return Status::Ok();
+}
+
+// Uniform separable axes, kx(c) = kx0 + c dkx and ky(r) = ky0 + r dky (the reference's
+// meshgrid of (-P/2 : P/2-1) / (P dx), ToTEM_submit_v1.m:1534-1538), on power-of-two grids admit
+// the gridding builder.  Its job table holds one job per species segment of every slice
+// (neutral, then ionic), in slice order.
+Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::SpeciesHost& spn,
+                                    const totem::SpeciesHost& spi) {
+  grid_ok = false;
+  grid_job_beg_h.clear();
+  grid_jobs_h.clear();
+  grid_atoms = 0;
+  if (!totem::fused_fft_size_ok(p_h) || !totem::fused_fft_size_ok(p_w) || slices <= 0) return Status::Ok();
+  auto uniform = [](const double* v, int n, long stride, double* d) {
+    *d = (v[(long)(n - 1) * stride] - v[0]) / (n - 1);
+    if (!std::isfinite(*d) || *d == 0.0) return false;
+    for (int i = 0; i < n; ++i)
+      if (!(std::fabs(v[(long)i * stride] - (v[0] + i * *d)) <= 1e-9 * std::fabs(*d))) return false;
+    return true;
+  };
+  double dkx = 0, dky = 0;
+  if (!uniform(a->kx, p_w, 1, &dkx) || !uniform(a->ky, p_h, p_w, &dky)) return Status::Ok();
+  grid_dkx = dkx;
+  grid_dky = dky;
+  grid_sx = a->kx[0] + dkx * (p_w / 2);
+  grid_sy = a->ky[0] + dky * (p_h / 2);
+  grid_job_beg_h.assign(slices + 1, 0);
+  for (int s = 0; s < slices; ++s) {
+    for (int kind = 0; kind < 2; ++kind) {
+      const totem::SpeciesHost& sp = kind ? spi : spn;
+      if ((int)sp.seg_beg.size() != slices + 1) continue;
+      for (int q = sp.seg_beg[s]; q < sp.seg_beg[s + 1]; ++q) {
+        grid_jobs_h.push_back(make_int4(kind, sp.seg[3 * q], sp.seg[3 * q + 1], sp.seg[3 * q + 2]));
+        grid_atoms += sp.seg[3 * q + 2] - sp.seg[3 * q + 1];
+      }
+    }
+    grid_job_beg_h[s + 1] = (int)grid_jobs_h.size();
+  }
+  cudaStream_t st = stream;
+  TOTEM_TRY(upload(grid_jobs, grid_jobs_h, st));
+  TOTEM_TRY(upload(grid_job_beg, grid_job_beg_h, st));
+  TOTEM_TRY(upload(grid_ax, totem::grid_deconvolution(p_w), st));
+  TOTEM_TRY(upload(grid_ay, totem::grid_deconvolution(p_h), st));
+  grid_ok = true;
+  return Status::Ok();
+}
+
+// Cost model of the two separable builders, measured on B200 (SrTiO3 supercells filling the
+// grid, 20 slices): the direct sums take ~0.29 ps per atom and pixel; gridding takes per job
+// (species and slice) and pixel 54 ps at 1024^2, 68 ps at 2048^2 and 100 ps at 4096^2 (the
+// long column transforms run below bandwidth), plus ~20 us of launches per batch.
+bool totem_session::gridding_cheaper() const {
+  const double plane = (double)p_h * p_w;
+  const double jobs = (double)grid_jobs_h.size();
+  const int edge = std::max(p_h, p_w);
+  const double per_px = edge <= 1024 ? 5.5e-11 : (edge <= 2048 ? 7.0e-11 : 1.0e-10);
+  const double per_batch =
+      std::max(1.0, std::floor((double)totem::tx_gridding_scratch() / (double)totem::grid_job_bytes(p_h, p_w)));
+  const double direct = 2.9e-13 * (double)grid_atoms * plane;
+  const double gridding = per_px * jobs * plane + 2e-5 * (std::ceil(jobs / per_batch) + 1);
+  return gridding < direct;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -903,6 +993,33 @@ int totem_stem_run(const TotemStemArgs* args, const TotemRunOptions* opt, TotemS
     TOTEM_TRY(s->run(0, opt));
     return s->download(out);
   });
+}
+
+int totem_set_tx_builder(int mode, size_t scratch_bytes) {
+  if (mode != TOTEM_TX_AUTO && mode != TOTEM_TX_DIRECT && mode != TOTEM_TX_GRIDDING)
+    return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "unknown transmission builder mode"));
+  g_tx_mode.store(mode);
+  g_tx_scratch.store(scratch_bytes);
+  g_last_error.clear();
+  return TOTEM_OK;
+}
+
+int totem_grid_batches(const int* job_beg, int slices, int jobs_per_batch, int* out, int max_batches, int* count) {
+  if (!job_beg || !out || !count || slices < 0 || jobs_per_batch < 1 || max_batches < 0)
+    return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "invalid batch-plan arguments"));
+  for (int s = 0; s < slices; ++s)
+    if (job_beg[s + 1] < job_beg[s] || job_beg[0] != 0)
+      return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "job_beg is not a prefix sum from 0"));
+  const auto b = totem::grid_batches(std::vector<int>(job_beg, job_beg + slices + 1), jobs_per_batch);
+  *count = (int)b.size();
+  for (int i = 0; i < (int)b.size() && i < max_batches; ++i) {
+    out[4 * i] = b[i].s_lo;
+    out[4 * i + 1] = b[i].s_hi;
+    out[4 * i + 2] = b[i].j_lo;
+    out[4 * i + 3] = b[i].j_hi;
+  }
+  g_last_error.clear();
+  return TOTEM_OK;
 }
 
 int totem_transmission_run(const TotemStemArgs* args, TotemStemOut* out) {

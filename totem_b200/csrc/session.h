@@ -163,6 +163,13 @@ struct totem_session {
   totem::DevBuf probe, prop, mask_mid, mask_exit, tw_n, tw_pw, tw_ph, gfsf_d;
   totem::RowsDev rows_n, rows_i, rows_cn, rows_ci;
   totem::SpeciesRowsDev species_n, species_i;  // the neutral / ionic rows by species (separable grids)
+  // gridding builder (uniform separable axes): job table, deconvolution tables, work memory
+  bool grid_ok = false;
+  double grid_dkx = 0, grid_dky = 0, grid_sx = 0, grid_sy = 0;
+  long long grid_atoms = 0;
+  std::vector<int> grid_job_beg_h;
+  std::vector<int4> grid_jobs_h;
+  totem::DevBuf grid_jobs, grid_job_beg, grid_ax, grid_ay, grid_scratch;
   totem::DevBuf kx_axis, ky_axis, kx, ky, s2, aper_true, cim;
   // work buffers and results
   totem::DevBuf T, psi, part, acc, out_result, out_mid;
@@ -199,7 +206,8 @@ struct totem_session {
   void for_each_buf(F&& f) {
     for (totem::DevBuf* b : {&probe, &prop, &mask_mid, &mask_exit, &tw_n, &tw_pw, &tw_ph, &gfsf_d, &kx_axis, &ky_axis,
                              &kx, &ky, &s2, &aper_true, &cim, &T, &psi, &part, &acc, &out_result, &out_mid,
-                             &ev_slice, &Tb, &hr_wave, &hr_prop, &hr_tf, &hr_w, &hr_work, &hr_exit, &hr_img})
+                             &ev_slice, &Tb, &hr_wave, &hr_prop, &hr_tf, &hr_w, &hr_work, &hr_exit, &hr_img, &grid_jobs,
+                             &grid_job_beg, &grid_ax, &grid_ay, &grid_scratch})
       f(*b);
     for (totem::RowsDev* r : {&rows_n, &rows_i, &rows_cn, &rows_ci})
       for (totem::DevBuf* b : {&r->pos, &r->coef, &r->absorp, &r->beg}) f(*b);
@@ -253,6 +261,8 @@ struct totem_session {
   static Status validate(const TotemStemArgs* a, bool stem);
   Status upload_args(const TotemStemArgs* a, bool stem);
   Status build_transmission(int path, int* launches);
+  Status plan_gridding(const TotemStemArgs* a, const totem::SpeciesHost& spn, const totem::SpeciesHost& spi);
+  bool gridding_cheaper() const;
   totem::DetectionEvents detection_events() const;
   // Per-event detector sums acc[event][w][A][depth] -> out_result (exit) and out_mid (layers),
   // weighted by gfsf over w (accumulate_result, cuda_source_lobato.cu:981-1015).

@@ -14,6 +14,9 @@
 //    reference's separable grids the two factors are tabulated per atom and tile;
 //  * the ifftshift before the inverse FFT is folded into a (-1)^(r+c) factor after it, and
 //    APERTURE is applied while the sum is written.
+#include <algorithm>
+#include <cmath>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -280,6 +283,181 @@ __global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesDev nr, 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// By species through Gaussian gridding (a type-1 non-uniform FFT), for uniform separable grids
+// kx(c) = kx0 + c dkx, ky(r) = ky0 + r dky.  With kx' = c - p_w/2, ky' = r - p_h/2,
+//   S(r, c) = sum_a w_a exp(-i (kx' tx_a + ky' ty_a)),
+//   tx_a = 2 pi frac(dkx x_a), ty_a = 2 pi frac(dky y_a),
+//   w_a = exp(-2 pi i (kx(p_w/2) x_a + ky(p_h/2) y_a))   (1 on centred grids).
+// Each atom is spread with a periodic Gaussian exp(-d^2 / (4 tau)) onto a grid twice as fine as
+// the potential (GR_W x GR_W points), the fine grid is transformed, and the Gaussian's transform
+// sqrt(pi / tau) exp(-k^2 tau) is divided out: Greengard & Lee, "Accelerating the nonuniform
+// fast Fourier transform", SIAM Review 46 (2004) 443-454, with oversampling R = 2, half-width
+// M_sp = 7 and tau = pi M_sp / (P^2 R (R - 1/2)).  The relative L2 error of S is ~1e-7 (below
+// the FP32 sums) whatever the atom count; the cost is O(atoms + P^2 log P) per species and
+// slice instead of O(atoms P^2).
+//
+// The 2P x 2P fine grid is held as four P x P planes by the parity of its indices, plane
+// (ey, ex) = points (2 qy + ey, 2 qx + ex), so its transform is four P x P FFTs and a half-bin
+// phase: F(k) = sum_{ey, ex} exp(-i pi (ky ey / p_h + kx ex / p_w)) FFT(plane_{ey,ex})[k mod P].
+// Atoms are added in 32.32 fixed point (64-bit integer atomics), so the grid, and everything
+// after it, is bit-reproducible whatever order the atomics land in.  The row FFT converts a
+// row to complex64 in place (the first half of its 16-byte-per-point storage), so the planes
+// keep a pitch of 2 p_w complex64 values from then on.
+// ---------------------------------------------------------------------------------------------
+constexpr int GR_MSP = 7;
+constexpr int GR_W = 2 * GR_MSP;
+constexpr float GR_FIX = 4294967296.f;         // 2^32
+constexpr float GR_UNFIX = 1.f / 4294967296.f;
+
+__global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, int p_w, const double* __restrict__ pos_n,
+                                                     const double* __restrict__ pos_i, int job0,
+                                                     unsigned long long* __restrict__ grid) {
+  const int4 jb = gp.jobs[job0 + blockIdx.y];  // kind, species, first atom, end atom
+  const double* pos = jb.x ? pos_i : pos_n;
+  const long plane = (long)p_h * p_w;
+  unsigned long long* base = grid + (long)blockIdx.y * 8 * plane;  // 4 planes of (re, im) pairs
+  const int total = (jb.w - jb.z) * GR_W;
+  // h^2 / (4 tau) for the fine-grid spacing h = 2 pi / (2P): pi (R - 1/2) / (R M_sp)
+  const float kappa = 3.f * 3.14159265358979f / (4.f * GR_MSP);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int q = t / GR_W, jy = t - q * GR_W;
+    const int a = jb.z + q;
+    const double x = pos[2L * a], y = pos[2L * a + 1];
+    const double fx = gp.dkx * x, fy = gp.dky * y;
+    const double u = (fx - floor(fx)) * (2.0 * p_w), v = (fy - floor(fy)) * (2.0 * p_h);
+    const double fu = floor(u), fv = floor(v);
+    const float du = (float)(u - fu), dv = (float)(v - fv);
+    const float2 w = phase_of(gp.sx * x + gp.sy * y);
+    const int my = ((int)fv + jy - (GR_MSP - 1)) & (2 * p_h - 1);
+    const float ey = (float)(jy - (GR_MSP - 1)) - dv;
+    unsigned long long* row = base + (long)(my & 1) * 4 * plane + (long)(my >> 1) * 2 * p_w;
+#pragma unroll 2
+    for (int jx = 0; jx < GR_W; ++jx) {
+      const int mx = ((int)fu + jx - (GR_MSP - 1)) & (2 * p_w - 1);
+      const float ex = (float)(jx - (GR_MSP - 1)) - du;
+      const float gw = __expf(-kappa * fmaf(ex, ex, ey * ey)) * GR_FIX;
+      unsigned long long* dst = row + (long)(mx & 1) * 2 * plane + 2 * (mx >> 1);
+      atomicAdd(dst, (unsigned long long)__float2ll_rn(w.x * gw));
+      atomicAdd(dst + 1, (unsigned long long)__float2ll_rn(w.y * gw));
+    }
+  }
+}
+
+// Forward FFT of fine-grid rows (p_w = N points of fixed-point pairs, 16 bytes each), written
+// back as complex64 into the first half of the row.
+// (A 128-register bound: the forward transform of a 16-byte-per-point row does not fit 96.)
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T,
+                                  (512 / (RowCfg<N>::G * RowCfg<N>::T) > 0) ? 512 / (RowCfg<N>::G * RowCfg<N>::T) : 1)
+    k_grid_rows(void* __restrict__ grid, const float2* __restrict__ tw) {
+  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T, G = RowCfg<N>::G;
+  extern __shared__ float2 sh[];
+  float2* s_tw = sh;
+  float2* s_x = sh + Fft<N>::tw_size;
+  const int g = threadIdx.x / T, j = threadIdx.x - g * T;
+  const long row = (long)blockIdx.x * G + g;
+  const longlong2* src = static_cast<const longlong2*>(grid) + row * N;
+  float2 v[P];
+#pragma unroll
+  for (int m = 0; m < P; ++m) {
+    const longlong2 q = src[j + m * T];
+    v[m] = make_float2(__ll2float_rn(q.x) * GR_UNFIX, __ll2float_rn(q.y) * GR_UNFIX);
+  }
+  load_twiddles<N>(s_tw, tw);
+  __syncthreads();  // every point of the CTA's rows is in registers before any is overwritten
+  fft_regs<N, false>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
+  float2* dst = static_cast<float2*>(grid) + row * 2 * N;
+#pragma unroll
+  for (int m = 0; m < P; ++m) dst[j + m * T] = v[m];
+}
+
+// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).
+template <int N>
+__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) k_grid_cols(float2* __restrict__ data,
+                                                                          int width, long pitch, long plane_stride,
+                                                                          const float2* __restrict__ tw) {
+  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
+  extern __shared__ float2 sh[];
+  float2* s_tw = sh;
+  float2* s_x = sh + Fft<N>::tw_size;
+  const int j = threadIdx.x / G, g = threadIdx.x - j * G;
+  const int nblk = width / G;
+  const long pl = blockIdx.x / nblk;
+  const int cb = blockIdx.x - (int)pl * nblk;
+  float2* p = data + pl * plane_stride + cb * G + g;
+  load_twiddles<N>(s_tw, tw);
+  float2 v[P];
+#pragma unroll
+  for (int m = 0; m < P; ++m) v[m] = p[(long)(j + m * T) * pitch];
+  __syncthreads();
+  fft_regs<N, false>(v, j, g, s_tw, s_x, ColLayout<N, G>(), SyncBlock());
+#pragma unroll
+  for (int m = 0; m < P; ++m) p[(long)(j + m * T) * pitch] = v[m];
+}
+
+// V(r, c) of slices s_lo.. from the transformed planes of jobs [j_lo, j_hi): per job the
+// half-bin combination and Gaussian deconvolution give S, then f_species(s^2) S is summed;
+// PARAMETER * APERTURE as in k_tx_species.  A slice whose first jobs ran in an earlier batch
+// adds to what that batch wrote.
+__global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, SpeciesDev ir, GridPlanDev gp,
+                                                      const float2* __restrict__ grid, int s_lo, int j_lo, int j_hi,
+                                                      float2* __restrict__ out) {
+  const long plane = (long)g.p_h * g.p_w;
+  const long pitch = 2L * g.p_w, pstride = (long)g.p_h * pitch;
+  const int s = s_lo + blockIdx.y;
+  const int jb0 = max(gp.job_beg[s], j_lo), jb1 = min(gp.job_beg[s + 1], j_hi);
+  const bool add = gp.job_beg[s] < j_lo;
+  float2* dst = out + (long)s * plane;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < plane; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / g.p_w), c = (int)(i - (long)r * g.p_w);
+    const int qr = (r + g.p_h / 2) & (g.p_h - 1), qc = (c + g.p_w / 2) & (g.p_w - 1);
+    const float2 x0 = gp.ax[2 * c], x1 = gp.ax[2 * c + 1], y0 = gp.ay[2 * r], y1 = gp.ay[2 * r + 1];
+    const float2 f00 = cmul(y0, x0), f01 = cmul(y0, x1), f10 = cmul(y1, x0), f11 = cmul(y1, x1);
+    const float s2 = g.s2[i];
+    float2 acc = make_float2(0.f, 0.f);
+    for (int jj = jb0; jj < jb1; ++jj) {
+      const int4 jb = gp.jobs[jj];
+      const float2* F = grid + (long)(jj - j_lo) * 4 * pstride + (long)qr * pitch + qc;
+      float2 S = cmul(f00, F[0]);
+      S = cadd(S, cmul(f01, F[pstride]));
+      S = cadd(S, cmul(f10, F[2 * pstride]));
+      S = cadd(S, cmul(f11, F[3 * pstride]));
+      const SpeciesDev& d = jb.x ? ir : nr;
+      float fr, fi;
+      row_form(jb.x, g.lobato, d.coef + (long)jb.y * d.ncoef, d.absorp != nullptr ? d.absorp + (long)jb.y * 10 : nullptr,
+               s2, fr, fi);
+      acc.x = fmaf(fr, S.x, fmaf(-fi, S.y, acc.x));
+      acc.y = fmaf(fr, S.y, fmaf(fi, S.x, acc.y));
+    }
+    const float ap = (g.aper_true != nullptr) ? g.aper_true[i] : 1.f;
+    float2 v = cscale(acc, g.parameter * ap);
+    if (add) v = cadd(dst[i], v);
+    dst[i] = v;
+  }
+}
+
+template <int N>
+Status grid_rows(void* grid, long nrows, const float2* tw, cudaStream_t st) {
+  constexpr int T = RowCfg<N>::T, G = RowCfg<N>::G;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_grid_rows<N>, smem));
+  if (nrows % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "row count not a multiple of the row tile");
+  k_grid_rows<N><<<(unsigned)(nrows / G), G * T, smem, st>>>(grid, tw);
+  return cuda_status(cudaGetLastError(), "k_grid_rows");
+}
+
+template <int N>
+Status grid_cols(float2* data, long planes, int width, long pitch, long plane_stride, const float2* tw,
+                 cudaStream_t st) {
+  constexpr int T = ColCfg<N>::T, G = ColCfg<N>::G;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_grid_cols<N>, smem));
+  if (width % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "grid width not a multiple of the column tile");
+  k_grid_cols<N><<<(unsigned)(planes * (width / G)), G * T, smem, st>>>(data, width, pitch, plane_stride, tw);
+  return cuda_status(cudaGetLastError(), "k_grid_cols");
+}
+
 // In-place inverse FFT of rows of length N (RowCfg<N>::G rows per CTA).
 template <int N>
 __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) k_fft_rows_inv(float2* __restrict__ data,
@@ -390,6 +568,98 @@ Status launch_tx_species(const TxGrid& g, const SpeciesDev& neutral, const Speci
   dim3 grid((g.p_w + SP_T - 1) / SP_T, (g.p_h + SP_T - 1) / SP_T, g.slices);
   k_tx_species<<<grid, 256, 0, st>>>(g, neutral, ion, out);
   return cuda_status(cudaGetLastError(), "k_tx_species");
+}
+
+std::vector<float2> grid_deconvolution(int n) {
+  // tau = pi M_sp / (n^2 R (R - 1/2)); the fine grid's FFT carries 1 / (R n) per axis
+  const double pi = 3.14159265358979323846;
+  const double tau = pi * GR_MSP / ((double)n * n * 2.0 * 1.5);
+  const double pre = std::sqrt(pi / tau) / (2.0 * n);
+  std::vector<float2> t(2 * (size_t)n);
+  for (int c = 0; c < n; ++c) {
+    const double k = c - n / 2;
+    const double d = pre * std::exp(k * k * tau);
+    t[2 * c] = make_float2((float)d, 0.f);
+    t[2 * c + 1] = make_float2((float)(d * std::cos(pi * k / n)), (float)(-d * std::sin(pi * k / n)));
+  }
+  return t;
+}
+
+std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_per_batch) {
+  std::vector<GridBatch> out;
+  const int slices = (int)job_beg.size() - 1;
+  if (slices <= 0 || jobs_per_batch < 1) return out;
+  const int total = job_beg[slices];
+  int s_lo = 0, j_lo = 0;
+  while (s_lo < slices) {
+    const int j_hi = std::min(j_lo + jobs_per_batch, total);
+    int s_hi = s_lo;
+    if (j_hi == total) s_hi = slices;
+    else
+      while (s_hi < slices && job_beg[s_hi] < j_hi) ++s_hi;
+    out.push_back(GridBatch{s_lo, s_hi, j_lo, j_hi});
+    const bool partial = job_beg[s_hi] > j_hi;  // slice s_hi - 1 continues in the next batch
+    s_lo = partial ? s_hi - 1 : s_hi;
+    j_lo = j_hi;
+  }
+  return out;
+}
+
+Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDev& ir, const GridPlanDev& gp,
+                          const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,
+                          const float2* tw_h, void* scratch, size_t scratch_bytes, float2* out, cudaStream_t st,
+                          int* launches) {
+  if (g.slices == 0) return Status::Ok();
+  if (!fused_fft_size_ok(g.p_h) || !fused_fft_size_ok(g.p_w))
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "gridding builder needs power-of-two grids 64..4096");
+  if ((int)job_beg.size() != g.slices + 1) return Status::Err(TOTEM_ERR_STATE, "gridding job table size");
+  const long plane = (long)g.p_h * g.p_w;
+  const size_t job_bytes = grid_job_bytes(g.p_h, g.p_w);
+  const int per_batch = (int)std::min<size_t>(scratch_bytes / job_bytes, 65535);  // grid.y of the spread
+  if (per_batch < 1) return Status::Err(TOTEM_ERR_STATE, "gridding scratch below one job");
+  const long pitch = 2L * g.p_w, pstride = (long)g.p_h * pitch;
+  for (const GridBatch& b : grid_batches(job_beg, per_batch)) {
+    const int nj = b.j_hi - b.j_lo;
+    if (nj > 0) {
+      TOTEM_CUDA(cudaMemsetAsync(scratch, 0, job_bytes * nj, st));
+      int most = 0;
+      for (int j = b.j_lo; j < b.j_hi; ++j) most = std::max(most, jobs[j].w - jobs[j].z);
+      const unsigned bx = (unsigned)std::min<long>(((long)most * GR_W + 255) / 256 + 1, 4096);
+      k_grid_spread<<<dim3(bx, nj), 256, 0, st>>>(gp, g.p_h, g.p_w, nr.pos, ir.pos, b.j_lo,
+                                                  static_cast<unsigned long long*>(scratch));
+      TOTEM_TRY(cuda_status(cudaGetLastError(), "k_grid_spread"));
+      const long rows = (long)nj * 4 * g.p_h, planes = (long)nj * 4;
+      float2* f = static_cast<float2*>(scratch);
+      switch (g.p_w) {
+        case 64: TOTEM_TRY(grid_rows<64>(scratch, rows, tw_w, st)); break;
+        case 128: TOTEM_TRY(grid_rows<128>(scratch, rows, tw_w, st)); break;
+        case 256: TOTEM_TRY(grid_rows<256>(scratch, rows, tw_w, st)); break;
+        case 512: TOTEM_TRY(grid_rows<512>(scratch, rows, tw_w, st)); break;
+        case 1024: TOTEM_TRY(grid_rows<1024>(scratch, rows, tw_w, st)); break;
+        case 2048: TOTEM_TRY(grid_rows<2048>(scratch, rows, tw_w, st)); break;
+        case 4096: TOTEM_TRY(grid_rows<4096>(scratch, rows, tw_w, st)); break;
+      }
+      switch (g.p_h) {
+        case 64: TOTEM_TRY(grid_cols<64>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 128: TOTEM_TRY(grid_cols<128>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 256: TOTEM_TRY(grid_cols<256>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 512: TOTEM_TRY(grid_cols<512>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 1024: TOTEM_TRY(grid_cols<1024>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 2048: TOTEM_TRY(grid_cols<2048>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 4096: TOTEM_TRY(grid_cols<4096>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+      }
+      *launches += 3;
+    }
+    const unsigned cx = (unsigned)std::min<long>((plane + 255) / 256, 2048);
+    for (int s0 = b.s_lo; s0 < b.s_hi; s0 += 65535) {
+      const int ns = std::min(b.s_hi - s0, 65535);
+      k_grid_combine<<<dim3(cx, ns), 256, 0, st>>>(g, nr, ir, gp, static_cast<const float2*>(scratch), s0, b.j_lo,
+                                                   b.j_hi, out);
+      TOTEM_TRY(cuda_status(cudaGetLastError(), "k_grid_combine"));
+      ++*launches;
+    }
+  }
+  return Status::Ok();
 }
 
 Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sig, const float2* tw_w,

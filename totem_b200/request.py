@@ -220,6 +220,72 @@ def with_absorption(req: StemRequest, seed: int = 1, scale: float = 0.05) -> Ste
                    absorp_n_i=rows(len(req.ele_n_i)) if len(req.ele_n_i) else None)
 
 
+def with_ionic_oxygen(req: StemRequest, every: int = 3, ion_fraction: float = 0.4) -> StemRequest:
+    """Move every ``every``-th neutral row to the ionic table as partly ionised O (O2-: the ion
+    fraction from the ionic Peng table, the rest neutral O), keeping per-slice counts (tests;
+    Peng requests only)."""
+    o2 = specimen.ion_params(8, -2)
+    neutral_o = specimen.element_params(8, "p")
+    rows = req.ele_n
+    n = len(rows)
+    ion_idx = np.arange(0, n, every)
+    ion_rows = np.zeros((len(ion_idx), 25))
+    ion_rows[:, 0:3] = rows[ion_idx, 0:3]
+    ion_rows[:, 3] = ion_fraction
+    ion_rows[:, 4:14:2], ion_rows[:, 5:14:2] = o2[:5], o2[5:]
+    ion_rows[:, 14] = 1.0 - ion_fraction
+    ion_rows[:, 15:25:2], ion_rows[:, 16:25:2] = neutral_o[:5], neutral_o[5:]
+    keep = np.setdiff1d(np.arange(n), ion_idx)
+    beg = np.concatenate([[0], np.cumsum(req.series_n)]).astype(int)
+    sl = np.searchsorted(beg, np.arange(n), side="right") - 1
+    series_n = np.bincount(sl[keep], minlength=req.slices).astype(float)
+    series_i = np.bincount(sl[ion_idx], minlength=req.slices).astype(float)
+    return replace(req, ele_n=rows[keep], series_n=series_n, ele_n_i=ion_rows, series_n_i=series_i)
+
+
+def with_correction(req: StemRequest, seed: int = 2, every: int = 4) -> StemRequest:
+    """Attach synthetic Peng-extended correction rows to a request (tests only): two correction
+    planes (cim) on the potential grid, a neutral row (x, y, B, amplitude, plane) at every
+    ``every``-th atom and an ionic row (x, y, B, amplitude, w1, plane1, w2, plane2) at every
+    ``2 every``-th, keeping the atoms' slices."""
+    rng = np.random.default_rng(seed)
+    cim = np.stack([np.exp(-req.s2 * rng.uniform(0.5, 3.0)) * rng.uniform(0.5, 1.5, size=req.s2.shape)
+                    for _ in range(2)])
+    beg = np.concatenate([[0], np.cumsum(req.series_n)]).astype(int)
+    n_rows, i_rows, n_cnt, i_cnt = [], [], np.zeros(req.slices), np.zeros(req.slices)
+    for k in range(req.slices):
+        for a in range(beg[k], beg[k + 1]):
+            x, y = req.ele_n[a, 0], req.ele_n[a, 1]
+            if a % every == 0:
+                n_rows.append([x, y, rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), 1 + a % 2])
+                n_cnt[k] += 1
+            if a % (2 * every) == 1:
+                i_rows.append([x, y, rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), rng.uniform(0, 1), 1,
+                               rng.uniform(0, 1), 2])
+                i_cnt[k] += 1
+    return replace(req, corr_info_matrix=cim, series_n_corr=n_cnt, series_n_i_corr=i_cnt,
+                   ele_n_corr=np.asarray(n_rows, dtype=float).reshape(-1, 5),
+                   ele_n_i_corr=np.asarray(i_rows, dtype=float).reshape(-1, 8))
+
+
+def without_slice_atoms(req: StemRequest, slices) -> StemRequest:
+    """The request with every atom of the given 0-based slices removed (vacuum slices; tests)."""
+    drop = set(int(s) for s in slices)
+
+    def cut(rows, counts, extra):
+        if rows is None or len(rows) == 0:
+            return rows, counts, extra
+        beg = np.concatenate([[0], np.cumsum(counts)]).astype(int)
+        keep = np.concatenate([np.arange(beg[s], beg[s + 1]) for s in range(len(counts)) if s not in drop]
+                              + [np.zeros(0, dtype=int)]).astype(int)
+        c = np.array([0.0 if s in drop else counts[s] for s in range(len(counts))])
+        return rows[keep], c, (extra[keep] if extra is not None else None)
+    ele_n, series_n, absorp_n = cut(req.ele_n, req.series_n, req.absorp_n)
+    ele_n_i, series_n_i, absorp_n_i = cut(req.ele_n_i, req.series_n_i, req.absorp_n_i)
+    return replace(req, ele_n=ele_n, series_n=series_n, absorp_n=absorp_n, ele_n_i=ele_n_i,
+                   series_n_i=series_n_i, absorp_n_i=absorp_n_i)
+
+
 # ----------------------------------------------------------------------------------------------
 # HRTEM (the reference's HRTEMsimulation: *P transmission, then plane-wave multislice and TCC
 # imaging in MATLAB, ToTEM_submit_v1.m:1259-1369)
