@@ -372,12 +372,14 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T,
   for (int m = 0; m < P; ++m) dst[j + m * T] = v[m];
 }
 
-// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).
+// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).  Columns of
+// 4096 take four per CTA (32-byte row segments, whole sectors; 168 KB of shared memory).
 template <int N>
-__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) k_grid_cols(float2* __restrict__ data,
-                                                                          int width, long pitch, long plane_stride,
-                                                                          const float2* __restrict__ tw) {
-  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
+using GridColCfg = ColCfg<N, 4, (N == 4096) ? 4 : 0>;
+template <int N>
+__global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCfg<N>::MINB)
+    k_grid_cols(float2* __restrict__ data, int width, long pitch, long plane_stride, const float2* __restrict__ tw) {
+  constexpr int P = GridColCfg<N>::P, T = GridColCfg<N>::T, G = GridColCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
@@ -450,7 +452,7 @@ Status grid_rows(void* grid, long nrows, const float2* tw, cudaStream_t st) {
 template <int N>
 Status grid_cols(float2* data, long planes, int width, long pitch, long plane_stride, const float2* tw,
                  cudaStream_t st) {
-  constexpr int T = ColCfg<N>::T, G = ColCfg<N>::G;
+  constexpr int T = GridColCfg<N>::T, G = GridColCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_grid_cols<N>, smem));
   if (width % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "grid width not a multiple of the column tile");
