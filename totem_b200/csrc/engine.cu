@@ -445,13 +445,13 @@ Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::Species
 
 // Cost model of the two separable builders, measured on B200 (SrTiO3 supercells filling the
 // grid, 20 slices): the direct sums take ~0.29 ps per atom and pixel; gridding takes per job
-// (species and slice) and pixel 54 ps at 1024^2, 68 ps at 2048^2 and 100 ps at 4096^2 (the
+// (species and slice) and pixel 42 ps at 1024^2, 53 ps at 2048^2 and 65 ps at 4096^2 (the
 // long column transforms run below bandwidth), plus ~20 us of launches per batch.
 bool totem_session::gridding_cheaper() const {
   const double plane = (double)p_h * p_w;
   const double jobs = (double)grid_jobs_h.size();
   const int edge = std::max(p_h, p_w);
-  const double per_px = edge <= 1024 ? 5.5e-11 : (edge <= 2048 ? 7.0e-11 : 1.0e-10);
+  const double per_px = edge <= 1024 ? 4.2e-11 : (edge <= 2048 ? 5.3e-11 : 6.5e-11);
   const double per_batch =
       std::max(1.0, std::floor((double)totem::tx_gridding_scratch() / (double)totem::grid_job_bytes(p_h, p_w)));
   const double direct = 2.9e-13 * (double)grid_atoms * plane;

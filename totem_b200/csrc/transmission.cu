@@ -300,10 +300,13 @@ __global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesDev nr, 
 // The 2P x 2P fine grid is held as four P x P planes by the parity of its indices, plane
 // (ey, ex) = points (2 qy + ey, 2 qx + ex), so its transform is four P x P FFTs and a half-bin
 // phase: F(k) = sum_{ey, ex} exp(-i pi (ky ey / p_h + kx ex / p_w)) FFT(plane_{ey,ex})[k mod P].
+// The x half of that sum is taken right after the row transforms (the rows of parity ex = 0
+// and 1 of a fine row pair share a CTA), together with the x deconvolution, so two planes per
+// job, ey = 0 and 1, go through the column transforms and the combine.
 // Atoms are added in 32.32 fixed point (64-bit integer atomics), so the grid, and everything
-// after it, is bit-reproducible whatever order the atomics land in.  The row FFT converts a
-// row to complex64 in place (the first half of its 16-byte-per-point storage), so the planes
-// keep a pitch of 2 p_w complex64 values from then on.
+// after it, is bit-reproducible whatever order the atomics land in.  The row pass writes its
+// complex64 output in place into the ex = 0 row (the first half of its 16-byte-per-point
+// storage), so the planes keep a pitch of 2 p_w complex64 values from then on.
 // ---------------------------------------------------------------------------------------------
 constexpr int GR_MSP = 7;
 constexpr int GR_W = 2 * GR_MSP;
@@ -344,20 +347,30 @@ __global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, in
   }
 }
 
-// Forward FFT of fine-grid rows (p_w = N points of fixed-point pairs, 16 bytes each), written
-// back as complex64 into the first half of the row.
-// (A 128-register bound: the forward transform of a 16-byte-per-point row does not fit 96.)
+// Row pass: forward FFTs of the fine-grid rows of parity ex = 0 and 1 of one (job, ey, qy)
+// (p_w = N points of fixed-point pairs, 16 bytes each) in one CTA, then
+//   out[c] = ax[c][0] FFT(row_0)[k] + ax[c][1] FFT(row_1)[k],  k = (c + N/2) mod N,
+// written as complex64 over the first half of the ex = 0 row.  Transform g of a CTA takes parity
+// g & 1; the partner's spectrum comes through shared memory.  (A 128-register bound: the
+// forward transform of a 16-byte-per-point row does not fit 96.)
 template <int N>
-__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T,
-                                  (512 / (RowCfg<N>::G * RowCfg<N>::T) > 0) ? 512 / (RowCfg<N>::G * RowCfg<N>::T) : 1)
-    k_grid_rows(void* __restrict__ grid, const float2* __restrict__ tw) {
-  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T, G = RowCfg<N>::G;
+struct GridRowCfg {
+  static constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T;
+  static constexpr int G = RowCfg<N>::G < 2 ? 2 : RowCfg<N>::G;
+  static constexpr int MINB = (512 / (G * T) > 0) ? 512 / (G * T) : 1;
+};
+template <int N>
+__global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCfg<N>::MINB)
+    k_grid_rows(void* __restrict__ grid, const float4* __restrict__ ax, int p_h, const float2* __restrict__ tw) {
+  constexpr int P = GridRowCfg<N>::P, T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
-  const int g = threadIdx.x / T, j = threadIdx.x - g * T;
-  const long row = (long)blockIdx.x * G + g;
-  const longlong2* src = static_cast<const longlong2*>(grid) + row * N;
+  const int g = threadIdx.x / T, j = threadIdx.x - g * T, ex = g & 1;
+  const long pair = (long)blockIdx.x * (G / 2) + (g >> 1);
+  const long qy = pair % p_h, t = pair / p_h;                 // t = 2 job + ey
+  const long row0 = ((t >> 1) * 4 + 2 * (t & 1)) * p_h + qy;  // plane (ey, 0), row qy
+  const longlong2* src = static_cast<const longlong2*>(grid) + (row0 + ex * p_h) * N;
   float2 v[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) {
@@ -367,9 +380,21 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T,
   load_twiddles<N>(s_tw, tw);
   __syncthreads();  // every point of the CTA's rows is in registers before any is overwritten
   fft_regs<N, false>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
-  float2* dst = static_cast<float2*>(grid) + row * 2 * N;
+  const RowLayout<N> L;
 #pragma unroll
-  for (int m = 0; m < P; ++m) dst[j + m * T] = v[m];
+  for (int m = 0; m < P; ++m) s_x[L(g, j + m * T)] = v[m];
+  __syncthreads();
+  float2* dst = static_cast<float2*>(grid) + row0 * 2 * N;
+#pragma unroll
+  for (int m = 0; m < P; ++m) {
+    if ((m < P / 2) != (ex == 0)) continue;  // parity 0 finishes k < N/2, parity 1 the rest
+    const int k = j + m * T;
+    const float2 other = s_x[L(g ^ 1, k)];
+    const float2 x0 = ex ? other : v[m], x1 = ex ? v[m] : other;
+    const int c = (k + N / 2) & (N - 1);
+    const float4 a = ax[c];
+    dst[c] = cadd(cmul(make_float2(a.x, a.y), x0), cmul(make_float2(a.z, a.w), x1));
+  }
 }
 
 // Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).  Columns of
@@ -398,10 +423,10 @@ __global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCf
   for (int m = 0; m < P; ++m) p[(long)(j + m * T) * pitch] = v[m];
 }
 
-// V(r, c) of slices s_lo.. from the transformed planes of jobs [j_lo, j_hi): per job the
-// half-bin combination and Gaussian deconvolution give S, then f_species(s^2) S is summed;
-// PARAMETER * APERTURE as in k_tx_species.  A slice whose first jobs ran in an earlier batch
-// adds to what that batch wrote.
+// V(r, c) of slices s_lo.. from the transformed planes of jobs [j_lo, j_hi): per job the y
+// half-bin combination and deconvolution give S, then f_species(s^2) S is summed; PARAMETER *
+// APERTURE as in k_tx_species.  A slice whose first jobs ran in an earlier batch adds to what
+// that batch wrote.
 __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, SpeciesDev ir, GridPlanDev gp,
                                                       const float2* __restrict__ grid, int s_lo, int j_lo, int j_hi,
                                                       float2* __restrict__ out) {
@@ -413,18 +438,14 @@ __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, S
   float2* dst = out + (long)s * plane;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < plane; i += (long)gridDim.x * blockDim.x) {
     const int r = (int)(i / g.p_w), c = (int)(i - (long)r * g.p_w);
-    const int qr = (r + g.p_h / 2) & (g.p_h - 1), qc = (c + g.p_w / 2) & (g.p_w - 1);
-    const float2 x0 = gp.ax[2 * c], x1 = gp.ax[2 * c + 1], y0 = gp.ay[2 * r], y1 = gp.ay[2 * r + 1];
-    const float2 f00 = cmul(y0, x0), f01 = cmul(y0, x1), f10 = cmul(y1, x0), f11 = cmul(y1, x1);
+    const int qr = (r + g.p_h / 2) & (g.p_h - 1);
+    const float2 y0 = gp.ay[2 * r], y1 = gp.ay[2 * r + 1];
     const float s2 = g.s2[i];
     float2 acc = make_float2(0.f, 0.f);
     for (int jj = jb0; jj < jb1; ++jj) {
       const int4 jb = gp.jobs[jj];
-      const float2* F = grid + (long)(jj - j_lo) * 4 * pstride + (long)qr * pitch + qc;
-      float2 S = cmul(f00, F[0]);
-      S = cadd(S, cmul(f01, F[pstride]));
-      S = cadd(S, cmul(f10, F[2 * pstride]));
-      S = cadd(S, cmul(f11, F[3 * pstride]));
+      const float2* F = grid + (long)(jj - j_lo) * 4 * pstride + (long)qr * pitch + c;
+      const float2 S = cadd(cmul(y0, F[0]), cmul(y1, F[2 * pstride]));
       const SpeciesDev& d = jb.x ? ir : nr;
       float fr, fi;
       row_form(jb.x, g.lobato, d.coef + (long)jb.y * d.ncoef, d.absorp != nullptr ? d.absorp + (long)jb.y * 10 : nullptr,
@@ -440,12 +461,12 @@ __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, S
 }
 
 template <int N>
-Status grid_rows(void* grid, long nrows, const float2* tw, cudaStream_t st) {
-  constexpr int T = RowCfg<N>::T, G = RowCfg<N>::G;
+Status grid_rows(void* grid, long pairs, const float2* ax, int p_h, const float2* tw, cudaStream_t st) {
+  constexpr int T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_grid_rows<N>, smem));
-  if (nrows % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "row count not a multiple of the row tile");
-  k_grid_rows<N><<<(unsigned)(nrows / G), G * T, smem, st>>>(grid, tw);
+  if (pairs % (G / 2)) return Status::Err(TOTEM_ERR_UNSUPPORTED, "row count not a multiple of the row tile");
+  k_grid_rows<N><<<(unsigned)(pairs / (G / 2)), G * T, smem, st>>>(grid, reinterpret_cast<const float4*>(ax), p_h, tw);
   return cuda_status(cudaGetLastError(), "k_grid_rows");
 }
 
@@ -630,25 +651,25 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
       k_grid_spread<<<dim3(bx, nj), 256, 0, st>>>(gp, g.p_h, g.p_w, nr.pos, ir.pos, b.j_lo,
                                                   static_cast<unsigned long long*>(scratch));
       TOTEM_TRY(cuda_status(cudaGetLastError(), "k_grid_spread"));
-      const long rows = (long)nj * 4 * g.p_h, planes = (long)nj * 4;
+      const long pairs = (long)nj * 2 * g.p_h, planes = (long)nj * 2;  // (job, ey) after the row pass
       float2* f = static_cast<float2*>(scratch);
       switch (g.p_w) {
-        case 64: TOTEM_TRY(grid_rows<64>(scratch, rows, tw_w, st)); break;
-        case 128: TOTEM_TRY(grid_rows<128>(scratch, rows, tw_w, st)); break;
-        case 256: TOTEM_TRY(grid_rows<256>(scratch, rows, tw_w, st)); break;
-        case 512: TOTEM_TRY(grid_rows<512>(scratch, rows, tw_w, st)); break;
-        case 1024: TOTEM_TRY(grid_rows<1024>(scratch, rows, tw_w, st)); break;
-        case 2048: TOTEM_TRY(grid_rows<2048>(scratch, rows, tw_w, st)); break;
-        case 4096: TOTEM_TRY(grid_rows<4096>(scratch, rows, tw_w, st)); break;
+        case 64: TOTEM_TRY(grid_rows<64>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 128: TOTEM_TRY(grid_rows<128>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 256: TOTEM_TRY(grid_rows<256>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 512: TOTEM_TRY(grid_rows<512>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 1024: TOTEM_TRY(grid_rows<1024>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 2048: TOTEM_TRY(grid_rows<2048>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 4096: TOTEM_TRY(grid_rows<4096>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
       }
       switch (g.p_h) {
-        case 64: TOTEM_TRY(grid_cols<64>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
-        case 128: TOTEM_TRY(grid_cols<128>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
-        case 256: TOTEM_TRY(grid_cols<256>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
-        case 512: TOTEM_TRY(grid_cols<512>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
-        case 1024: TOTEM_TRY(grid_cols<1024>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
-        case 2048: TOTEM_TRY(grid_cols<2048>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
-        case 4096: TOTEM_TRY(grid_cols<4096>(f, planes, g.p_w, pitch, pstride, tw_h, st)); break;
+        case 64: TOTEM_TRY(grid_cols<64>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 128: TOTEM_TRY(grid_cols<128>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 256: TOTEM_TRY(grid_cols<256>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 512: TOTEM_TRY(grid_cols<512>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 1024: TOTEM_TRY(grid_cols<1024>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 2048: TOTEM_TRY(grid_cols<2048>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 4096: TOTEM_TRY(grid_cols<4096>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
       }
       *launches += 3;
     }
