@@ -27,9 +27,10 @@ def _both(req, scratch_bytes=0):
     return direct, grid
 
 
-@pytest.mark.parametrize("flag", ["p", "l"])
-def test_gridding_vs_oracle(engine_lib, flag):
-    req = request.build_small_stem(flag=flag)
+@pytest.mark.parametrize("flag,p", [("p", 128), ("l", 128), ("p", 256)])
+def test_gridding_vs_oracle(engine_lib, flag, p):
+    # from 256 on, the row pass skips fine rows no atom touched
+    req = request.build_small_stem(flag=flag, p=p)
     direct, grid = _both(req)
     ref = so.transmission(req)
     assert rel_l2(grid, ref) < TOL, rel_l2(grid, ref)
@@ -64,7 +65,7 @@ def test_gridding_batches_split_slices(engine_lib):
     # scratch for one job: every slice's species run in separate batches, later ones adding to
     # what the earlier ones wrote; equal to the unsplit build up to FP32 rounding
     req = request.with_ionic_oxygen(request.build_small_stem(flag="p"))
-    one_job = req.p_height * req.p_width * 64
+    one_job = req.p_height * req.p_width * 64 + 8 * req.p_height  # four planes and the row flags
     _, whole = _both(req)
     _, split = _both(req, scratch_bytes=one_job)
     _, three = _both(req, scratch_bytes=3 * one_job)

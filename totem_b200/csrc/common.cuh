@@ -116,8 +116,8 @@ struct GridBatch {
   int s_lo, s_hi, j_lo, j_hi;
 };
 std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_per_batch);
-// Scratch of one job: four p_h x p_w planes of 16-byte points.
-inline size_t grid_job_bytes(int p_h, int p_w) { return (size_t)p_h * p_w * 64; }
+// Scratch of one job: four p_h x p_w planes of 16-byte points and a flag per fine row.
+inline size_t grid_job_bytes(int p_h, int p_w) { return (size_t)p_h * p_w * 64 + (size_t)p_h * 8; }
 // Overwrites out like launch_tx_species; ``scratch`` holds at least one job.
 Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, const GridPlanDev& gp,
                           const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,

@@ -353,9 +353,10 @@ Status totem_session::build_transmission(int path, int* launches) {
     const auto si = species_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
     const int mode = totem::tx_builder_mode();
     if (grid_ok && (mode == TOTEM_TX_GRIDDING || (mode == TOTEM_TX_AUTO && gridding_cheaper()))) {
-      const size_t job = totem::grid_job_bytes(p_h, p_w);
+      // jobs per batch from the budget for their planes (64 bytes per pixel); the row flags on top
       const size_t jobs = std::max<size_t>(grid_jobs_h.size(), 1);
-      const size_t bytes = std::max<size_t>(1, std::min(totem::tx_gridding_scratch() / job, jobs)) * job;
+      const size_t per = std::min(totem::tx_gridding_scratch() / ((size_t)p_h * p_w * 64), jobs);
+      const size_t bytes = std::max<size_t>(1, per) * totem::grid_job_bytes(p_h, p_w);
       TOTEM_TRY(grid_scratch.ensure(bytes));
       totem::GridPlanDev gp;
       gp.dkx = grid_dkx; gp.dky = grid_dky; gp.sx = grid_sx; gp.sy = grid_sy;
@@ -445,15 +446,14 @@ Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::Species
 
 // Cost model of the two separable builders, measured on B200 (SrTiO3 supercells filling the
 // grid, 20 slices): the direct sums take ~0.29 ps per atom and pixel; gridding takes per job
-// (species and slice) and pixel 42 ps at 1024^2, 53 ps at 2048^2 and 65 ps at 4096^2 (the
+// (species and slice) and pixel 33 ps at 1024^2, 41 ps at 2048^2 and 48 ps at 4096^2 (the
 // long column transforms run below bandwidth), plus ~20 us of launches per batch.
 bool totem_session::gridding_cheaper() const {
   const double plane = (double)p_h * p_w;
   const double jobs = (double)grid_jobs_h.size();
   const int edge = std::max(p_h, p_w);
-  const double per_px = edge <= 1024 ? 4.2e-11 : (edge <= 2048 ? 5.3e-11 : 6.5e-11);
-  const double per_batch =
-      std::max(1.0, std::floor((double)totem::tx_gridding_scratch() / (double)totem::grid_job_bytes(p_h, p_w)));
+  const double per_px = edge <= 1024 ? 3.3e-11 : (edge <= 2048 ? 4.1e-11 : 4.8e-11);
+  const double per_batch = std::max(1.0, std::floor((double)totem::tx_gridding_scratch() / (plane * 64.0)));
   const double direct = 2.9e-13 * (double)grid_atoms * plane;
   const double gridding = per_px * jobs * plane + 2e-5 * (std::ceil(jobs / per_batch) + 1);
   return gridding < direct;

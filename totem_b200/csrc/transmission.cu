@@ -315,7 +315,8 @@ constexpr float GR_UNFIX = 1.f / 4294967296.f;
 
 __global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, int p_w, const double* __restrict__ pos_n,
                                                      const double* __restrict__ pos_i, int job0,
-                                                     unsigned long long* __restrict__ grid) {
+                                                     unsigned long long* __restrict__ grid,
+                                                     unsigned* __restrict__ row_used) {
   const int4 jb = gp.jobs[job0 + blockIdx.y];  // kind, species, first atom, end atom
   const double* pos = jb.x ? pos_i : pos_n;
   const long plane = (long)p_h * p_w;
@@ -333,6 +334,7 @@ __global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, in
     const float du = (float)(u - fu), dv = (float)(v - fv);
     const float2 w = phase_of(gp.sx * x + gp.sy * y);
     const int my = ((int)fv + jy - (GR_MSP - 1)) & (2 * p_h - 1);
+    row_used[(long)blockIdx.y * 2 * p_h + my] = 1u;  // the row pass skips fine rows nobody touched
     const float ey = (float)(jy - (GR_MSP - 1)) - dv;
     unsigned long long* row = base + (long)(my & 1) * 4 * plane + (long)(my >> 1) * 2 * p_w;
 #pragma unroll 2
@@ -351,8 +353,11 @@ __global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, in
 // (p_w = N points of fixed-point pairs, 16 bytes each) in one CTA, then
 //   out[c] = ax[c][0] FFT(row_0)[k] + ax[c][1] FFT(row_1)[k],  k = (c + N/2) mod N,
 // written as complex64 over the first half of the ex = 0 row.  Transform g of a CTA takes parity
-// g & 1; the partner's spectrum comes through shared memory.  (A 128-register bound: the
-// forward transform of a 16-byte-per-point row does not fit 96.)
+// g & 1; the partner's spectrum comes through shared memory.  A fine row that no atom touched
+// (row_used == 0; most rows of a crystal, whose atoms sit on lattice rows) is zero and so is its
+// transform: the pair skips all work (from N = 256, where a pair never shares a warp with
+// another pair's warp-level barriers).  (A 128-register bound: the forward transform of a
+// 16-byte-per-point row does not fit 96.)
 template <int N>
 struct GridRowCfg {
   static constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T;
@@ -361,7 +366,8 @@ struct GridRowCfg {
 };
 template <int N>
 __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCfg<N>::MINB)
-    k_grid_rows(void* __restrict__ grid, const float4* __restrict__ ax, int p_h, const float2* __restrict__ tw) {
+    k_grid_rows(void* __restrict__ grid, const unsigned* __restrict__ row_used, const float4* __restrict__ ax, int p_h,
+                const float2* __restrict__ tw) {
   constexpr int P = GridRowCfg<N>::P, T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
@@ -370,20 +376,27 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   const long pair = (long)blockIdx.x * (G / 2) + (g >> 1);
   const long qy = pair % p_h, t = pair / p_h;                 // t = 2 job + ey
   const long row0 = ((t >> 1) * 4 + 2 * (t & 1)) * p_h + qy;  // plane (ey, 0), row qy
+  // fine row 2 qy + ey of job t / 2
+  const bool live = N < 256 || row_used[(t >> 1) * 2 * p_h + 2 * qy + (t & 1)] != 0u;
   const longlong2* src = static_cast<const longlong2*>(grid) + (row0 + ex * p_h) * N;
   float2 v[P];
+  if (live) {
 #pragma unroll
-  for (int m = 0; m < P; ++m) {
-    const longlong2 q = src[j + m * T];
-    v[m] = make_float2(__ll2float_rn(q.x) * GR_UNFIX, __ll2float_rn(q.y) * GR_UNFIX);
+    for (int m = 0; m < P; ++m) {
+      const longlong2 q = src[j + m * T];
+      v[m] = make_float2(__ll2float_rn(q.x) * GR_UNFIX, __ll2float_rn(q.y) * GR_UNFIX);
+    }
   }
   load_twiddles<N>(s_tw, tw);
   __syncthreads();  // every point of the CTA's rows is in registers before any is overwritten
-  fft_regs<N, false>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
   const RowLayout<N> L;
+  if (live) {
+    fft_regs<N, false>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
 #pragma unroll
-  for (int m = 0; m < P; ++m) s_x[L(g, j + m * T)] = v[m];
+    for (int m = 0; m < P; ++m) s_x[L(g, j + m * T)] = v[m];
+  }
   __syncthreads();
+  if (!live) return;  // the output row is still the zero the grid was cleared to
   float2* dst = static_cast<float2*>(grid) + row0 * 2 * N;
 #pragma unroll
   for (int m = 0; m < P; ++m) {
@@ -397,10 +410,11 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   }
 }
 
-// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).  Columns of
-// 4096 take four per CTA (32-byte row segments, whole sectors; 168 KB of shared memory).
+// Column shape of the builder's transforms: columns of 4096 take four per CTA (32-byte row
+// segments, whole sectors; 168 KB of shared memory), shorter ones the default width.
 template <int N>
 using GridColCfg = ColCfg<N, 4, (N == 4096) ? 4 : 0>;
+// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).
 template <int N>
 __global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCfg<N>::MINB)
     k_grid_cols(float2* __restrict__ data, int width, long pitch, long plane_stride, const float2* __restrict__ tw) {
@@ -461,12 +475,14 @@ __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, S
 }
 
 template <int N>
-Status grid_rows(void* grid, long pairs, const float2* ax, int p_h, const float2* tw, cudaStream_t st) {
+Status grid_rows(void* grid, const unsigned* row_used, long pairs, const float2* ax, int p_h, const float2* tw,
+                 cudaStream_t st) {
   constexpr int T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_grid_rows<N>, smem));
   if (pairs % (G / 2)) return Status::Err(TOTEM_ERR_UNSUPPORTED, "row count not a multiple of the row tile");
-  k_grid_rows<N><<<(unsigned)(pairs / (G / 2)), G * T, smem, st>>>(grid, reinterpret_cast<const float4*>(ax), p_h, tw);
+  k_grid_rows<N><<<(unsigned)(pairs / (G / 2)), G * T, smem, st>>>(grid, row_used, reinterpret_cast<const float4*>(ax),
+                                                                   p_h, tw);
   return cuda_status(cudaGetLastError(), "k_grid_rows");
 }
 
@@ -504,9 +520,9 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) 
 
 // Column inverse FFT of length N over a p_w-wide plane, (-1)^(r+c), exp(i s V).
 template <int N>
-__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB) k_fft_cols_exp(float2* __restrict__ data, int p_w,
+__global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCfg<N>::MINB) k_fft_cols_exp(float2* __restrict__ data, int p_w,
                                                                              const float2* __restrict__ tw, float sig) {
-  constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T, G = ColCfg<N>::G;
+  constexpr int P = GridColCfg<N>::P, T = GridColCfg<N>::T, G = GridColCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
@@ -562,7 +578,7 @@ Status rows_inv(float2* data, long nrows, const float2* tw, cudaStream_t st) {
 
 template <int N>
 Status cols_exp(float2* data, int slices, int p_w, const float2* tw, float sig, cudaStream_t st) {
-  constexpr int T = ColCfg<N>::T, G = ColCfg<N>::G;
+  constexpr int T = GridColCfg<N>::T, G = GridColCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_fft_cols_exp<N>, smem));
   if (p_w % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "potential width not a multiple of the column tile");
@@ -641,26 +657,29 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
   const int per_batch = (int)std::min<size_t>(scratch_bytes / job_bytes, 65535);  // grid.y of the spread
   if (per_batch < 1) return Status::Err(TOTEM_ERR_STATE, "gridding scratch below one job");
   const long pitch = 2L * g.p_w, pstride = (long)g.p_h * pitch;
+  const size_t plane_bytes = (size_t)plane * 64;  // four planes of 16-byte points per job
+  unsigned* used = reinterpret_cast<unsigned*>(static_cast<char*>(scratch) + plane_bytes * per_batch);
   for (const GridBatch& b : grid_batches(job_beg, per_batch)) {
     const int nj = b.j_hi - b.j_lo;
     if (nj > 0) {
-      TOTEM_CUDA(cudaMemsetAsync(scratch, 0, job_bytes * nj, st));
+      TOTEM_CUDA(cudaMemsetAsync(scratch, 0, plane_bytes * nj, st));
+      TOTEM_CUDA(cudaMemsetAsync(used, 0, sizeof(unsigned) * 2 * g.p_h * nj, st));
       int most = 0;
       for (int j = b.j_lo; j < b.j_hi; ++j) most = std::max(most, jobs[j].w - jobs[j].z);
       const unsigned bx = (unsigned)std::min<long>(((long)most * GR_W + 255) / 256 + 1, 4096);
       k_grid_spread<<<dim3(bx, nj), 256, 0, st>>>(gp, g.p_h, g.p_w, nr.pos, ir.pos, b.j_lo,
-                                                  static_cast<unsigned long long*>(scratch));
+                                                  static_cast<unsigned long long*>(scratch), used);
       TOTEM_TRY(cuda_status(cudaGetLastError(), "k_grid_spread"));
       const long pairs = (long)nj * 2 * g.p_h, planes = (long)nj * 2;  // (job, ey) after the row pass
       float2* f = static_cast<float2*>(scratch);
       switch (g.p_w) {
-        case 64: TOTEM_TRY(grid_rows<64>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
-        case 128: TOTEM_TRY(grid_rows<128>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
-        case 256: TOTEM_TRY(grid_rows<256>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
-        case 512: TOTEM_TRY(grid_rows<512>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
-        case 1024: TOTEM_TRY(grid_rows<1024>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
-        case 2048: TOTEM_TRY(grid_rows<2048>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
-        case 4096: TOTEM_TRY(grid_rows<4096>(scratch, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 64: TOTEM_TRY(grid_rows<64>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 128: TOTEM_TRY(grid_rows<128>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 256: TOTEM_TRY(grid_rows<256>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 512: TOTEM_TRY(grid_rows<512>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 1024: TOTEM_TRY(grid_rows<1024>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 2048: TOTEM_TRY(grid_rows<2048>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
+        case 4096: TOTEM_TRY(grid_rows<4096>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
       }
       switch (g.p_h) {
         case 64: TOTEM_TRY(grid_cols<64>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
