@@ -80,6 +80,22 @@ def test_gridding_is_deterministic(engine_lib):
     assert np.array_equal(a, b)  # fixed-point spreading: no dependence on atomic order
 
 
+def test_gridding_scratch_reuse_across_grids(engine_lib):
+    # the kernels leave the work memory cleared for the next build; builds of other grid sizes
+    # and batch splits in between must not change a result by a bit
+    a = request.build_small_stem(flag="p", p=256)
+    b = request.with_ionic_oxygen(request.build_small_stem(flag="p", p=128))
+    _, ta = _both(a)
+    _, tb = _both(b, scratch_bytes=b.p_height * b.p_width * 64)
+    for req, ref, scratch in ((a, ta, 0), (b, tb, 0), (a, ta, 3 * a.p_height * a.p_width * 64), (b, tb, 0)):
+        _, t = _both(req, scratch_bytes=scratch)
+        if scratch == 0 and req is a:
+            assert np.array_equal(t, ref)
+        else:
+            assert rel_l2(t, ref) < 1e-6
+    assert rel_l2(ta, so.transmission(a)) < TOL
+
+
 def test_gridding_needs_uniform_axes(engine_lib):
     # separable but non-uniform reciprocal axes: the gridding request falls back to the direct sums
     req = request.build_small_stem(flag="p")

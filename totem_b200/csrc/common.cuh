@@ -118,11 +118,12 @@ struct GridBatch {
 std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_per_batch);
 // Scratch of one job: four p_h x p_w planes of 16-byte points and a flag per fine row.
 inline size_t grid_job_bytes(int p_h, int p_w) { return (size_t)p_h * p_w * 64 + (size_t)p_h * 8; }
-// Overwrites out like launch_tx_species; ``scratch`` holds at least one job.
+// Overwrites out like launch_tx_species; ``scratch`` holds at least one job.  ``scratch_zero``:
+// the scratch is as an earlier call left it (otherwise it is cleared whole first).
 Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, const GridPlanDev& gp,
                           const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,
-                          const float2* tw_h, void* scratch, size_t scratch_bytes, float2* out, cudaStream_t st,
-                          int* launches);
+                          const float2* tw_h, void* scratch, size_t scratch_bytes, bool scratch_zero, float2* out,
+                          cudaStream_t st, int* launches);
 // Per-axis factors of the gridding builder for an axis of n points: [c][parity] = the inverse
 // of the spreading Gaussian's transform (normalised) times exp(-i pi k parity / n), k = c - n/2.
 std::vector<float2> grid_deconvolution(int n);

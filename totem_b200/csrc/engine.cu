@@ -357,16 +357,27 @@ Status totem_session::build_transmission(int path, int* launches) {
       const size_t jobs = std::max<size_t>(grid_jobs_h.size(), 1);
       const size_t per = std::min(totem::tx_gridding_scratch() / ((size_t)p_h * p_w * 64), jobs);
       const size_t bytes = std::max<size_t>(1, per) * totem::grid_job_bytes(p_h, p_w);
+      // the state the kernels leave the scratch in depends on the row layout and the batch size
+      const long long layout = ((long long)p_h << 40) | ((long long)p_w << 20) | (long long)std::max<size_t>(1, per);
+      if (bytes > grid_scratch.cap || layout != grid_scratch_layout) grid_scratch_zero = false;
       TOTEM_TRY(grid_scratch.ensure(bytes));
+      grid_scratch_layout = layout;
       totem::GridPlanDev gp;
       gp.dkx = grid_dkx; gp.dky = grid_dky; gp.sx = grid_sx; gp.sy = grid_sy;
       gp.ax = grid_ax.as<float2>(); gp.ay = grid_ay.as<float2>();
       gp.jobs = grid_jobs.as<int4>(); gp.job_beg = grid_job_beg.as<int>();
+      const bool was_zero = grid_scratch_zero;
+      grid_scratch_zero = false;  // until every batch has been enqueued
       TOTEM_TRY(totem::launch_tx_gridding(g, sn, si, gp, grid_job_beg_h, grid_jobs_h, tw_pw.as<float2>(),
-                                          tw_ph.as<float2>(), grid_scratch.p, bytes, T.as<float2>(), stream, launches));
+                                          tw_ph.as<float2>(), grid_scratch.p, bytes, was_zero, T.as<float2>(), stream,
+                                          launches));
+      grid_scratch_zero = true;  // left as the next build expects it (in stream order)
       // work memory of the build only: returned at once to a server's pool (stream-ordered and
-      // cheap); a plain session keeps it for its next build (cudaFree would synchronise)
-      if (grid_scratch.pool) grid_scratch.release();
+      // cheap); a plain session keeps it, cleared, for its next build (cudaFree would synchronise)
+      if (grid_scratch.pool) {
+        grid_scratch.release();
+        grid_scratch_zero = false;
+      }
     } else {
       TOTEM_TRY(totem::launch_tx_species(g, sn, si, T.as<float2>(), stream));
       ++*launches;
@@ -446,13 +457,13 @@ Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::Species
 
 // Cost model of the two separable builders, measured on B200 (SrTiO3 supercells filling the
 // grid, 20 slices): the direct sums take ~0.29 ps per atom and pixel; gridding takes per job
-// (species and slice) and pixel 33 ps at 1024^2, 41 ps at 2048^2 and 48 ps at 4096^2 (the
+// (species and slice) and pixel 29 ps at 1024^2, 35 ps at 2048^2 and 44 ps at 4096^2 (the
 // long column transforms run below bandwidth), plus ~20 us of launches per batch.
 bool totem_session::gridding_cheaper() const {
   const double plane = (double)p_h * p_w;
   const double jobs = (double)grid_jobs_h.size();
   const int edge = std::max(p_h, p_w);
-  const double per_px = edge <= 1024 ? 3.3e-11 : (edge <= 2048 ? 4.1e-11 : 4.8e-11);
+  const double per_px = edge <= 1024 ? 2.9e-11 : (edge <= 2048 ? 3.5e-11 : 4.4e-11);
   const double per_batch = std::max(1.0, std::floor((double)totem::tx_gridding_scratch() / (plane * 64.0)));
   const double direct = 2.9e-13 * (double)grid_atoms * plane;
   const double gridding = per_px * jobs * plane + 2e-5 * (std::ceil(jobs / per_batch) + 1);

@@ -165,6 +165,8 @@ struct totem_session {
   totem::SpeciesRowsDev species_n, species_i;  // the neutral / ionic rows by species (separable grids)
   // gridding builder (uniform separable axes): job table, deconvolution tables, work memory
   bool grid_ok = false;
+  bool grid_scratch_zero = false;  // grid_scratch is as the last gridding build left it, for
+  long long grid_scratch_layout = -1;  // that build's grid and jobs per batch
   double grid_dkx = 0, grid_dky = 0, grid_sx = 0, grid_sy = 0;
   long long grid_atoms = 0;
   std::vector<int> grid_job_beg_h;

@@ -356,8 +356,10 @@ __global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, in
 // g & 1; the partner's spectrum comes through shared memory.  A fine row that no atom touched
 // (row_used == 0; most rows of a crystal, whose atoms sit on lattice rows) is zero and so is its
 // transform: the pair skips all work (from N = 256, where a pair never shares a warp with
-// another pair's warp-level barriers).  (A 128-register bound: the forward transform of a
-// 16-byte-per-point row does not fit 96.)
+// another pair's warp-level barriers).  A pair that ran zeroes the second half of both its rows
+// and its flag; the first halves of all rows (where the column pass writes) are cleared in bulk
+// before each batch.  (A 128-register bound: the forward transform of a 16-byte-per-point row
+// does not fit 96.)
 template <int N>
 struct GridRowCfg {
   static constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T;
@@ -366,7 +368,7 @@ struct GridRowCfg {
 };
 template <int N>
 __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCfg<N>::MINB)
-    k_grid_rows(void* __restrict__ grid, const unsigned* __restrict__ row_used, const float4* __restrict__ ax, int p_h,
+    k_grid_rows(void* __restrict__ grid, unsigned* __restrict__ row_used, const float4* __restrict__ ax, int p_h,
                 const float2* __restrict__ tw) {
   constexpr int P = GridRowCfg<N>::P, T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   extern __shared__ float2 sh[];
@@ -377,8 +379,9 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   const long qy = pair % p_h, t = pair / p_h;                 // t = 2 job + ey
   const long row0 = ((t >> 1) * 4 + 2 * (t & 1)) * p_h + qy;  // plane (ey, 0), row qy
   // fine row 2 qy + ey of job t / 2
-  const bool live = N < 256 || row_used[(t >> 1) * 2 * p_h + 2 * qy + (t & 1)] != 0u;
-  const longlong2* src = static_cast<const longlong2*>(grid) + (row0 + ex * p_h) * N;
+  unsigned* flag = row_used + (t >> 1) * 2 * p_h + 2 * qy + (t & 1);
+  const bool live = N < 256 || *flag != 0u;
+  longlong2* src = static_cast<longlong2*>(grid) + (row0 + ex * p_h) * N;
   float2 v[P];
   if (live) {
 #pragma unroll
@@ -391,6 +394,10 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   __syncthreads();  // every point of the CTA's rows is in registers before any is overwritten
   const RowLayout<N> L;
   if (live) {
+    // clear what the next batch's bulk clear leaves out: the second half of both rows, and the flag
+    if (j == 0 && ex == 0) *flag = 0u;
+#pragma unroll
+    for (int m = P / 2; m < P; ++m) src[j + m * T] = make_longlong2(0, 0);
     fft_regs<N, false>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
 #pragma unroll
     for (int m = 0; m < P; ++m) s_x[L(g, j + m * T)] = v[m];
@@ -475,7 +482,7 @@ __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, S
 }
 
 template <int N>
-Status grid_rows(void* grid, const unsigned* row_used, long pairs, const float2* ax, int p_h, const float2* tw,
+Status grid_rows(void* grid, unsigned* row_used, long pairs, const float2* ax, int p_h, const float2* tw,
                  cudaStream_t st) {
   constexpr int T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
@@ -646,8 +653,8 @@ std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_pe
 
 Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDev& ir, const GridPlanDev& gp,
                           const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,
-                          const float2* tw_h, void* scratch, size_t scratch_bytes, float2* out, cudaStream_t st,
-                          int* launches) {
+                          const float2* tw_h, void* scratch, size_t scratch_bytes, bool scratch_zero, float2* out,
+                          cudaStream_t st, int* launches) {
   if (g.slices == 0) return Status::Ok();
   if (!fused_fft_size_ok(g.p_h) || !fused_fft_size_ok(g.p_w))
     return Status::Err(TOTEM_ERR_UNSUPPORTED, "gridding builder needs power-of-two grids 64..4096");
@@ -659,11 +666,15 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
   const long pitch = 2L * g.p_w, pstride = (long)g.p_h * pitch;
   const size_t plane_bytes = (size_t)plane * 64;  // four planes of 16-byte points per job
   unsigned* used = reinterpret_cast<unsigned*>(static_cast<char*>(scratch) + plane_bytes * per_batch);
+  // Between batches the kernels leave the second half of every fine row and the row flags zero;
+  // new scratch is cleared whole once, and the first halves (dense after the column pass) are
+  // cleared in bulk before each batch (a strided memset; clearing them in the combine after
+  // reading was measured 7x slower than the combine itself).
+  if (!scratch_zero) TOTEM_CUDA(cudaMemsetAsync(scratch, 0, job_bytes * per_batch, st));
   for (const GridBatch& b : grid_batches(job_beg, per_batch)) {
     const int nj = b.j_hi - b.j_lo;
     if (nj > 0) {
-      TOTEM_CUDA(cudaMemsetAsync(scratch, 0, plane_bytes * nj, st));
-      TOTEM_CUDA(cudaMemsetAsync(used, 0, sizeof(unsigned) * 2 * g.p_h * nj, st));
+      TOTEM_CUDA(cudaMemset2DAsync(scratch, 16 * (size_t)g.p_w, 0, 8 * (size_t)g.p_w, 4 * (size_t)g.p_h * nj, st));
       int most = 0;
       for (int j = b.j_lo; j < b.j_hi; ++j) most = std::max(most, jobs[j].w - jobs[j].z);
       const unsigned bx = (unsigned)std::min<long>(((long)most * GR_W + 255) / 256 + 1, 4096);
