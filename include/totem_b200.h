@@ -194,6 +194,39 @@ TOTEM_API int totem_set_tx_builder(int mode, size_t scratch_bytes);
 TOTEM_API int totem_grid_batches(const int *job_beg, int slices, int jobs_per_batch, int *out, int max_batches,
                                  int *count);
 
+/*
+ * Specimen preparation (host only, no device needed): the coefficient rows above from atom
+ * tables, as ToTem's MATLAB prepares them.
+ *
+ * Tables, one row per atom (getpotentialpara_lotabo_peng.m:26-84):
+ *   nuclear, 16 columns: Z x y z B occ a1 b1 .. a5 b5
+ *   nuc_ion, 28 columns: Z x y z B occ f_ion a1 b1 .. a5 b5 (ion) f_atom a1 b1 .. a5 b5 (atom)
+ *
+ * totem_slice_rows: slice assignment with erf weights; replaces
+ * CalAllEquilent20210223_lobato_peng.m:23-228.  Slice i spans slicethick[i] .. + eachthick; an
+ * atom within multiceng slices of it adds the share of its projected potential that falls inside
+ * (|erf(2 pi z2/sqrt(b))/2 - erf(2 pi z1/sqrt(b))/2| on every a_i).  Writes the rows
+ * (13/14 or 25/26 columns, TOTEM_PARAM_* layout; Lobato rows end with B * dbmode) slice by slice
+ * into ele_n / ele_n_i (capacity cap_n / cap_i rows; NULL to count only), the per-slice counts
+ * into series_n / series_n_i (slices entries each, or NULL), and the row totals into rows_n /
+ * rows_i.  Returns TOTEM_ERR_INVALID_ARG when a capacity is too small (the totals are still set).
+ */
+TOTEM_API int totem_slice_rows(int param, const double *nuclear, int n_nuclear, const double *nuc_ion, int n_ion,
+                               double eachthick, const double *slicethick, int slices, int multiceng, int dbmode,
+                               double *ele_n, long long cap_n, double *ele_n_i, long long cap_i, double *series_n,
+                               double *series_n_i, long long *rows_n, long long *rows_i);
+/* Debye-Waller B added to every Peng b_i, in place (CommonPart_forsimulation_lobato_peng.m:88-110);
+ * Lobato tables are left as they are (the engine applies exp(-B s^2) from the row's last column). */
+TOTEM_API int totem_fold_debye_waller(int param, double *nuclear, int n_nuclear, double *nuc_ion, int n_ion);
+/* One frozen-phonon configuration (randshiftpos.m:1-44): x, y, z (columns 1-3) of every row of
+ * an n x ncol table displaced by normal deviates of sigma = sqrt(B / 8 pi^2) (B in column 4),
+ * whole positions re-drawn while z leaves [slicethick[0], slicethick[slices-1] + eachthick).
+ * The deviates are a function of (seed, row, draw): a configuration is reproducible from its
+ * seed (the reference uses rng('shuffle')).  An atom still outside after 100 000 draws is an
+ * error. */
+TOTEM_API int totem_frozen_phonon(const double *table, int n, int ncol, double eachthick, const double *slicethick,
+                                  int slices, unsigned long long seed, double *out);
+
 /* Size of the fixed device scratch array used by totem_stem_slices_noalloc (per GPU). */
 #define TOTEM_NOALLOC_SCRATCH_BYTES (32ull << 20)
 

@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
                      "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", INCLUDE]
 CU_SOURCES = ["util.cu", "transmission.cu", "multislice.cu", "hrtem.cu", "optics.cu", "plain.cu", "engine.cu",
-              "noalloc.cu", "server.cu"]
+              "noalloc.cu", "server.cu", "specimen.cpp"]
 SHIMS = {  # library name -> (param flag, transmission flag)
     "libwaveCudaPeng.so": (0, 0),
     "libwaveCudaLobato.so": (1, 0),

@@ -150,6 +150,11 @@ def load() -> C.CDLL:
     lib.totem_tcc_stack.argtypes = [C.POINTER(TotemAberrations), C.c_double, C.c_int, C.c_double, C.c_double,
                                     C.c_int, C.c_int, C.c_double, _dp, _dp]
     lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
+    llp = C.POINTER(C.c_longlong)
+    lib.totem_slice_rows.argtypes = [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_double, _dp, C.c_int, C.c_int, C.c_int,
+                                     _dp, C.c_longlong, _dp, C.c_longlong, _dp, _dp, llp, llp]
+    lib.totem_fold_debye_waller.argtypes = [C.c_int, _dp, C.c_int, _dp, C.c_int]
+    lib.totem_frozen_phonon.argtypes = [_dp, C.c_int, C.c_int, C.c_double, _dp, C.c_int, C.c_ulonglong, _dp]
     lib.totem_grid_batches.argtypes = [_ip, C.c_int, C.c_int, _ip, C.c_int, _ip]
     lib.totem_plan_simulate.argtypes = [C.c_int, _ip, C.POINTER(C.c_longlong), _ip, _ip, ull, ull, C.c_int, _ip, _ip,
                                         ullp]
@@ -159,7 +164,7 @@ def load() -> C.CDLL:
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
-                 "totem_grid_batches"):
+                 "totem_grid_batches", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -476,6 +481,59 @@ def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
     opt = TotemRunOptions(path, batch, 0, 0, 0, T_COMPLEX64)
     check(lib.totem_stem_run(C.byref(m.args), C.byref(opt), C.byref(out)))
     return res, mid
+
+
+# ----------------------------------------------------------------------------------------------
+# Specimen preparation in the library (host only)
+# ----------------------------------------------------------------------------------------------
+
+def _param(flag: str) -> int:
+    return PARAM_LOBATO if flag == "l" else PARAM_PENG
+
+
+def _table(t, ncol):
+    t = np.ascontiguousarray(t, dtype=np.float64).reshape(-1, ncol)
+    return t, t.ctypes.data_as(_dp)
+
+
+def slice_rows(all_nuclear, all_nuc_ion, eachthick: float, slicethick, multiceng: int, flag: str, dbmode: int = 0):
+    """``totem_slice_rows``: the same outputs as ``specimen.slice_rows`` (ele_n, ele_n_i,
+    series_n, series_n_i; a kind without atoms gives an empty series)."""
+    lib = load()
+    nuc, nuc_p = _table(all_nuclear, 16)
+    ion, ion_p = _table(all_nuc_ion, 28)
+    st = np.ascontiguousarray(slicethick, dtype=np.float64)
+    S = len(st)
+    rn, ri = C.c_longlong(0), C.c_longlong(0)
+    args = (_param(flag), nuc_p, len(nuc), ion_p, len(ion), float(eachthick), st.ctypes.data_as(_dp), S,
+            int(multiceng), int(dbmode))
+    check(lib.totem_slice_rows(*args, None, 0, None, 0, None, None, C.byref(rn), C.byref(ri)))
+    extra = 1 if flag == "l" else 0
+    ele_n = np.zeros((rn.value, 13 + extra))
+    ele_i = np.zeros((ri.value, 25 + extra))
+    sn, si = np.zeros(S), np.zeros(S)
+    check(lib.totem_slice_rows(*args, ele_n.ctypes.data_as(_dp), rn.value, ele_i.ctypes.data_as(_dp), ri.value,
+                               sn.ctypes.data_as(_dp), si.ctypes.data_as(_dp), C.byref(rn), C.byref(ri)))
+    return ele_n, ele_i, (sn if len(nuc) else np.zeros(0)), (si if len(ion) else np.zeros(0))
+
+
+def fold_debye_waller(all_nuclear, all_nuc_ion, flag: str):
+    """``totem_fold_debye_waller`` on copies of the two tables."""
+    nuc, nuc_p = _table(np.array(all_nuclear, dtype=np.float64, copy=True), 16)
+    ion, ion_p = _table(np.array(all_nuc_ion, dtype=np.float64, copy=True), 28)
+    check(load().totem_fold_debye_waller(_param(flag), nuc_p, len(nuc), ion_p, len(ion)))
+    return nuc, ion
+
+
+def frozen_phonon(table, eachthick: float, slicethick, seed: int) -> np.ndarray:
+    """``totem_frozen_phonon``: one seeded thermal configuration of a 16/28-column table."""
+    t = np.ascontiguousarray(table, dtype=np.float64)
+    out = np.empty_like(t)
+    st = np.ascontiguousarray(slicethick, dtype=np.float64)
+    check(load().totem_frozen_phonon(t.ctypes.data_as(_dp), t.shape[0], t.shape[1], float(eachthick),
+                                     st.ctypes.data_as(_dp), len(st), int(seed) & (2 ** 64 - 1),
+                                     out.ctypes.data_as(_dp)))
+    return out
 
 
 TX_AUTO, TX_DIRECT, TX_GRIDDING = 0, 1, 2

@@ -122,10 +122,15 @@ def validate(req: StemRequest):
 def _stem_request(structure: specimen.Structure, flag: str, kv: float, sampling: float, n: int,
                   p: int, step: int, raster: tuple, begin: tuple, detectors_mrad, probe_spec,
                   mid_layer=(), dbmode: int = 0, multiceng: int = 0, engine_optics: bool = False,
-                  optics_from: Optional[StemRequest] = None) -> StemRequest:
+                  optics_from: Optional[StemRequest] = None, native_slicing: bool = False) -> StemRequest:
     nuc, ion = specimen.potential_params(structure.atoms, flag)
-    ele_n, ele_n_i, series_n, series_n_i = specimen.slice_rows(
-        nuc, ion, structure.slice_dz, structure.slicethick, multiceng, flag, dbmode)
+    if native_slicing:  # the library's slicer (totem_slice_rows): same rows, O(atoms) instead of O(atoms x slices)
+        from . import capi
+        ele_n, ele_n_i, series_n, series_n_i = capi.slice_rows(
+            nuc, ion, structure.slice_dz, structure.slicethick, multiceng, flag, dbmode)
+    else:
+        ele_n, ele_n_i, series_n, series_n_i = specimen.slice_rows(
+            nuc, ion, structure.slice_dz, structure.slicethick, multiceng, flag, dbmode)
     kx, ky, s2 = optics.reciprocal_grids(p, p, sampling)
     if optics_from is not None:  # same probe, detectors and propagator (e.g. another phonon configuration)
         probe, gfsf, aper, aper2, prop = (optics_from.probe, optics_from.gfsf, optics_from.aper, optics_from.aper2,
@@ -151,14 +156,15 @@ def build_srtio3_stem(cells=(8, 8, 50), n: int = 512, sampling: float = 0.0625, 
                       semi_angle: float = 25.0, c3_um: float = -5.0, defocus_nm: float = 0.0,
                       detectors=((60.0, 200.0), (0.0, 10.0)), mid_layer=(),
                       phonon_seed: Optional[int] = None, rms=None, engine_optics: bool = False,
-                      optics_from: Optional[StemRequest] = None) -> StemRequest:
+                      optics_from: Optional[StemRequest] = None, native_slicing: bool = False) -> StemRequest:
     """The SrTiO3 [001] STEM-ADF workload (8x8x50 cells, Peng, 300 kV, 512^2 window).
 
     The potential grid holds the scan plus one window: ``p = n + (raster-1)*step`` rounded up to a
     power of two, the block centred in it.  ``phonon_seed`` displaces atoms with per-element rms
     (Sr 0.089, Ti 0.075, O 0.088 Angstrom by default) drawn from ``numpy.random.default_rng(seed)``.
     ``engine_optics`` forms the probe's transfer functions on the GPU; ``optics_from`` reuses the
-    probe, detectors and propagator of an earlier request of the same optics.
+    probe, detectors and propagator of an earlier request of the same optics; ``native_slicing``
+    slices with the library (``totem_slice_rows``) instead of NumPy.
     """
     need = n + (max(raster) - 1) * step
     if p is None:
@@ -178,7 +184,8 @@ def build_srtio3_stem(cells=(8, 8, 50), n: int = 512, sampling: float = 0.0625, 
         atoms[:, 1:4] = moved[:, 1:4]
         st = specimen.Structure(atoms, st.extent, st.slice_dz, st.n_slices)
     return _stem_request(st, flag, kv, sampling, n, p, step, raster, begin, detectors, spec,
-                         mid_layer=mid_layer, engine_optics=engine_optics, optics_from=optics_from)
+                         mid_layer=mid_layer, engine_optics=engine_optics, optics_from=optics_from,
+                         native_slicing=native_slicing)
 
 
 def build_small_stem(n: int = 64, p: int = 128, raster=(3, 4), step: int = 5, slices: int = 6,

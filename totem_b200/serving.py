@@ -34,7 +34,7 @@ def _base(n: int, flag: str, rmax: int, smax: int):
     p = _grid(n, rmax)
     cells = max(1, int(p * SAMPLING // 3.905))
     return request.build_srtio3_stem(cells=(cells, cells, (smax + 1) // 2), n=n, sampling=SAMPLING, step=STEP,
-                                     raster=(rmax, rmax), p=p, flag=flag)
+                                     raster=(rmax, rmax), p=p, flag=flag, native_slicing=True)
 
 
 def derive(base, rows: int, cols: int, slices: int, mid_layer=()):

@@ -22,7 +22,7 @@ SAMPLING = 0.0625  # Angstrom per pixel
 def grid_filling_request(p: int, slices: int, flag: str = request.PENG):
     cells = max(1, int(p * SAMPLING // 3.905))
     return request.build_srtio3_stem(cells=(cells, cells, (slices + 1) // 2), n=64, raster=(1, 1), p=p,
-                                     sampling=SAMPLING, flag=flag)
+                                     sampling=SAMPLING, flag=flag, native_slicing=True)
 
 
 def build_ms(req, mode: int, reps: int) -> tuple[float, int]:
