@@ -137,12 +137,16 @@ def main(argv=None):
     ap.add_argument("--load", type=float, default=0.85, help="offered load as a fraction of burst capacity")
     ap.add_argument("--policy", default="shortest", choices=["fifo", "shortest"])
     ap.add_argument("--wave-mib", type=int, default=0, help="wave memory of the server (0 = its default)")
+    ap.add_argument("--chunk-mib", type=int, default=0, help="probes a request may start per tick (0 = default)")
     ap.add_argument("--prep-threads", type=int, default=0, help="server preparation threads (0 = its default)")
     ap.add_argument("--compare", action="store_true", help="also serve one request at a time")
+    ap.add_argument("--burst-only", action="store_true", help="skip the Poisson-arrival runs")
     ns = ap.parse_args(argv)
     policy = capi.SCHED_SHORTEST if ns.policy == "shortest" else capi.SCHED_FIFO
     reqs = make_workload(ns.requests, ns.seed, tuple(ns.sizes), ns.max_probes, tuple(ns.slices))
     kw = {"wave_bytes": ns.wave_mib << 20} if ns.wave_mib else {}
+    if ns.chunk_mib:
+        kw["chunk_bytes"] = ns.chunk_mib << 20
     if ns.prep_threads:
         kw["prep_threads"] = ns.prep_threads
     # warm-up (kernels, pools) on a few requests, then the burst capacity
@@ -152,6 +156,10 @@ def main(argv=None):
     if ns.compare:
         _, lat_sb, mk_sb = serve_one_at_a_time(reqs, np.zeros(len(reqs)))
         out.append(summary("one-at-a-time burst", reqs, lat_sb, mk_sb))
+    if ns.burst_only:
+        for o in out:
+            print(json.dumps(o), flush=True)
+        return out
     rate = ns.rate or ns.load * len(reqs) / mk_b
     arr = poisson_arrivals(len(reqs), rate, ns.seed)
     res_p, lat_p, mk_p = serve(reqs, arr, policy, **kw)
