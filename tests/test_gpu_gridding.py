@@ -38,6 +38,21 @@ def test_gridding_vs_oracle(engine_lib, flag, p):
     assert not np.array_equal(grid, direct)  # the gridding path ran
 
 
+def test_gridding_rectangular_grid(engine_lib):
+    # 128 rows x 256 columns: separate axis tables and transform lengths per direction
+    from totem_b200 import optics, specimen
+    st = specimen.center_in_field(specimen.srtio3_001(6, 3, 2), 256 * 0.2, 128 * 0.2)
+    req = request.specimen_request(st, "p", 200.0, 0.2, 128)
+    kx, ky, s2 = optics.reciprocal_grids(128, 256, 0.2)
+    req = replace(req, kx=kx, ky=ky, s2=s2, p_height=128, p_width=256, aper_true=np.ones((128, 256)),
+                  parameter=optics.potential_parameter(128, 256, 0.2))
+    direct, grid = _both(req)
+    ref = so.transmission(req)
+    assert grid.shape == (req.slices, 128, 256)
+    assert rel_l2(grid, ref) < TOL, rel_l2(grid, ref)
+    assert rel_l2(grid, direct) < TOL_DIRECT
+
+
 def test_gridding_ionic_absorptive_and_vacuum_slices(engine_lib):
     req = request.with_absorption(request.with_ionic_oxygen(request.build_small_stem(flag="p")))
     req = request.without_slice_atoms(req, [0, 3])
