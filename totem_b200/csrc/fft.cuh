@@ -439,8 +439,9 @@ struct RowCfg {
   static constexpr int G = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
   // resident CTAs of 128 threads requested per SM: 5 caps registers at 96 per thread, which
   // the padded exchange addressing fits without spilling up to N = 1024 (and 5 CTAs is also
-  // what the row pass's shared memory allows)
-  static constexpr int CTAS128 = (N <= 1024) ? 5 : 4;
+  // what the row pass's shared memory allows); from N = 2048 (three-stage transforms) 3, i.e.
+  // ~170 registers: the 2048 row pass spilled 200 B at 128 and ran 22 % slower
+  static constexpr int CTAS128 = (N <= 1024) ? 5 : 3;
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };
 // Columns: G adjacent columns per CTA, thread (j, g) = (tid / G, tid % G), so a warp's loads
@@ -448,8 +449,9 @@ struct RowCfg {
 template <int N, int CTAS128 = 4, int GW = 0>
 struct ColCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
-  // GW = 0: the default width, 16 columns (one 128-byte segment per row) up to N = 512
-  static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 1024 ? 8 : (N <= 2048 ? 4 : 2)));
+  // GW = 0: the default width, 16 columns (one 128-byte segment per row) up to N = 512, 8 (64
+  // bytes) up to 2048 (at 2048 one 512-thread CTA per SM; 4 columns at two CTAs was 10 % slower)
+  static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 2048 ? 8 : 2));
   // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };

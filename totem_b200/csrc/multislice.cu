@@ -331,7 +331,7 @@ Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
 }
 
 // Column-pass variants: 0/1 default; 2 propagator prefetched to shared memory; 3 a cap of
-// 6 x 128 threads per SM (80 registers at 16 columns); 5 tiles of 8 columns (up to N = 1024);
+// 6 x 128 threads per SM (80 registers at 16 columns); 5 tiles of 8 columns (up to N = 2048);
 // 6 tiles of 32 columns (up to N = 512).  col_blocks() gives the number of column tiles, i.e. of
 // detector partial sums per probe, of each variant.
 template <int N>
@@ -339,7 +339,7 @@ Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   switch (a.col_variant) {
     case 2: return col_pass_v<N, true, 4, 0>(a, flags, st);
     case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4), 0>(a, flags, st);
-    case 5: return col_pass_v<N, false, 4, (N <= 1024 ? 8 : 0)>(a, flags, st);
+    case 5: return col_pass_v<N, false, 4, (N <= 2048 ? 8 : 0)>(a, flags, st);
     case 6: return col_pass_v<N, false, 4, (N <= 512 ? 32 : 0)>(a, flags, st);
     default: return col_pass_v<N, false, 4, 0>(a, flags, st);
   }
@@ -347,7 +347,7 @@ Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
 
 template <int N>
 int col_tiles(int variant) {
-  if (N <= 1024 && variant == 5) return N / 8;
+  if (N <= 2048 && variant == 5) return N / 8;
   if (N <= 512 && variant == 6) return N / 32;
   return N / ColCfg<N>::G;
 }
