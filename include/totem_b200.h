@@ -186,6 +186,11 @@ TOTEM_API int totem_transmission_run(const TotemStemArgs *args, TotemStemOut *ou
 #define TOTEM_TX_DIRECT 1
 #define TOTEM_TX_GRIDDING 2
 TOTEM_API int totem_set_tx_builder(int mode, size_t scratch_bytes);
+/* Repeated runs of a session's fused slice loop with the same shapes and buffers replay as one
+ * CUDA graph (captured on the second such run): 1 = on (default), 0 = off.  Process-wide; no
+ * counterpart in the reference.  Runs on the legacy default stream, or on a stream the caller is
+ * capturing, are never graphed. */
+TOTEM_API int totem_set_slice_graphs(int enable);
 /* The gridding builder's batch plan, without a device (tests): jobs are numbered in slice order,
  * slice s owning jobs [job_beg[s], job_beg[s+1]); at most jobs_per_batch jobs run per batch.
  * Writes up to max_batches rows (s_lo, s_hi, j_lo, j_hi) to ``out`` and the batch count to

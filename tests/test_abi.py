@@ -107,3 +107,9 @@ def test_builder_choice_is_validated(lib):
     assert lib.totem_set_tx_builder(7, 0) == capi.ERR_INVALID_ARG
     assert lib.totem_set_tx_builder(capi.TX_GRIDDING, 1 << 20) == capi.OK
     assert lib.totem_set_tx_builder(capi.TX_AUTO, 0) == capi.OK
+
+
+def test_slice_graph_switch_is_validated(lib):
+    assert lib.totem_set_slice_graphs(2) == capi.ERR_INVALID_ARG
+    assert lib.totem_set_slice_graphs(0) == capi.OK
+    assert lib.totem_set_slice_graphs(1) == capi.OK

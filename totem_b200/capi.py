@@ -150,6 +150,7 @@ def load() -> C.CDLL:
     lib.totem_tcc_stack.argtypes = [C.POINTER(TotemAberrations), C.c_double, C.c_int, C.c_double, C.c_double,
                                     C.c_int, C.c_int, C.c_double, _dp, _dp]
     lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
+    lib.totem_set_slice_graphs.argtypes = [C.c_int]
     llp = C.POINTER(C.c_longlong)
     lib.totem_slice_rows.argtypes = [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_double, _dp, C.c_int, C.c_int, C.c_int,
                                      _dp, C.c_longlong, _dp, C.c_longlong, _dp, _dp, llp, llp]
@@ -164,7 +165,7 @@ def load() -> C.CDLL:
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
-                 "totem_grid_batches", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
+                 "totem_grid_batches", "totem_set_slice_graphs", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -537,6 +538,11 @@ def frozen_phonon(table, eachthick: float, slicethick, seed: int) -> np.ndarray:
 
 
 TX_AUTO, TX_DIRECT, TX_GRIDDING = 0, 1, 2
+
+
+def set_slice_graphs(enable: bool):
+    """``totem_set_slice_graphs``: replay repeated fused slice loops as CUDA graphs (default on)."""
+    check(load().totem_set_slice_graphs(1 if enable else 0))
 
 
 def set_tx_builder(mode: int, scratch_bytes: int = 0):

@@ -129,6 +129,8 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& neutral, const Spec
 std::vector<float2> grid_deconvolution(int n);
 // Process-wide builder choice for separable grids (TOTEM_TX_*) and gridding scratch bytes.
 int tx_builder_mode();
+// Process-wide: repeated fused slice loops replay as CUDA graphs (totem_set_slice_graphs).
+bool slice_graphs_enabled();
 size_t tx_gridding_scratch();
 // In-place unnormalised inverse 2-D FFT of every slice, times (-1)^(r+c) (the ifftshift of the
 // input), then T = exp(i * sigma_scaled * V).  Powers of two only; returns

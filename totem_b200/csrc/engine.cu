@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -36,6 +37,7 @@ namespace {
 
 thread_local std::string g_last_error;
 std::atomic<int> g_tx_mode{TOTEM_TX_AUTO};
+std::atomic<int> g_slice_graphs{1};
 std::atomic<size_t> g_tx_scratch{0};
 
 int fail(const Status& s) {
@@ -135,6 +137,7 @@ totem::SpeciesHost group_species(const RowsHost& h, int slices) {
 void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
 
 int totem::tx_builder_mode() { return g_tx_mode.load(); }
+bool totem::slice_graphs_enabled() { return g_slice_graphs.load() != 0; }
 size_t totem::tx_gridding_scratch() {
   const size_t b = g_tx_scratch.load();
   return b ? b : (1ull << 30);
@@ -526,7 +529,6 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   TOTEM_TRY(psi.ensure((size_t)B * vol * sizeof(float2)));
   TOTEM_TRY(part.ensure((size_t)n_events * B * aper_num * nblk * sizeof(double)));
   TOTEM_TRY(acc.ensure((size_t)n_events * w_num * ad * sizeof(double)));
-  TOTEM_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)n_events * w_num * ad * sizeof(double), stream));
   double* part_e = part.as<double>();
   const size_t part_stride = (size_t)B * aper_num * nblk;
   totem::ScanGeom geo{begin_row, begin_col, step, width_red, depth, p_w};
@@ -540,77 +542,149 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   }
   auto tslice = [&](int k) { return static_cast<const char*>(Tslices) + (size_t)k * tslice_bytes; };
 
-  for (long item0 = 0; item0 < items_total; item0 += B) {
-    const int items = (int)std::min<long>(B, items_total - item0);
-    if (fused) {
-      totem::SliceLoopArgs s;
-      s.n = h; s.items = items; s.item0 = (int)item0; s.geo = geo; s.p_h = p_h;
-      s.psi = psi.as<float2>(); s.probe = probe.as<float2>(); s.prop = prop.as<float2>();
-      s.tw = tw_n.as<float2>(); s.aper_num = aper_num;
-      s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
-      s.col_variant = col_variant;
-      s.t_bf16 = (t_storage == TOTEM_T_BF16);
-      TOTEM_TRY(prof_begin());
-      TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
-      TOTEM_TRY(prof_end(0));
-      ++*launches;
-      for (int k = 0; k < slices; ++k) {
-        const int ev_mid = event_of_slice[k + 1];
-        int flags = 0;
-        if (ev_mid >= 0) {
-          flags |= 1;
-          s.part_mid = part_e + ev_mid * part_stride;
-        }
-        if (k == slices - 1) {
-          flags |= 2 | 4;
-          s.part_exit = part_e + exit_event * part_stride;
-        }
+  // Everything below is stream work only (no allocation, no host synchronisation), so a repeated
+  // fused run can replay it as one CUDA graph (see run_graphed).
+  auto enqueue = [&]() -> Status {
+    TOTEM_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)n_events * w_num * ad * sizeof(double), stream));
+    for (long item0 = 0; item0 < items_total; item0 += B) {
+      const int items = (int)std::min<long>(B, items_total - item0);
+      if (fused) {
+        totem::SliceLoopArgs s;
+        s.n = h; s.items = items; s.item0 = (int)item0; s.geo = geo; s.p_h = p_h;
+        s.psi = psi.as<float2>(); s.probe = probe.as<float2>(); s.prop = prop.as<float2>();
+        s.tw = tw_n.as<float2>(); s.aper_num = aper_num;
+        s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
+        s.col_variant = col_variant;
+        s.t_bf16 = (t_storage == TOTEM_T_BF16);
         TOTEM_TRY(prof_begin());
-        TOTEM_TRY(totem::launch_col_pass(s, flags, stream));
-        TOTEM_TRY(prof_end(1));
+        TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
+        TOTEM_TRY(prof_end(0));
         ++*launches;
-        if (k < slices - 1) {
+        for (int k = 0; k < slices; ++k) {
+          const int ev_mid = event_of_slice[k + 1];
+          int flags = 0;
+          if (ev_mid >= 0) {
+            flags |= 1;
+            s.part_mid = part_e + ev_mid * part_stride;
+          }
+          if (k == slices - 1) {
+            flags |= 2 | 4;
+            s.part_exit = part_e + exit_event * part_stride;
+          }
           TOTEM_TRY(prof_begin());
-          TOTEM_TRY(totem::launch_row_pass(s, tslice(k + 1), false, stream));
-          TOTEM_TRY(prof_end(0));
+          TOTEM_TRY(totem::launch_col_pass(s, flags, stream));
+          TOTEM_TRY(prof_end(1));
           ++*launches;
+          if (k < slices - 1) {
+            TOTEM_TRY(prof_begin());
+            TOTEM_TRY(totem::launch_row_pass(s, tslice(k + 1), false, stream));
+            TOTEM_TRY(prof_end(0));
+            ++*launches;
+          }
         }
-      }
-    } else {
-      cufftHandle p;
-      TOTEM_TRY(plan(h, w, items, &p));
-      float2* ps = psi.as<float2>();
-      TOTEM_TRY(totem::launch_plain_init(ps, probe.as<float2>(), h, w, items, (int)item0, depth, stream));
-      ++*launches;
-      for (int k = 0; k < slices; ++k) {
-        TOTEM_TRY(totem::launch_plain_gather_mul(ps, Tp + (size_t)k * plane, h, w, items, (int)item0, geo, stream));
+      } else {
+        cufftHandle p;
+        TOTEM_TRY(plan(h, w, items, &p));
+        float2* ps = psi.as<float2>();
+        TOTEM_TRY(totem::launch_plain_init(ps, probe.as<float2>(), h, w, items, (int)item0, depth, stream));
+        ++*launches;
+        for (int k = 0; k < slices; ++k) {
+          TOTEM_TRY(totem::launch_plain_gather_mul(ps, Tp + (size_t)k * plane, h, w, items, (int)item0, geo, stream));
+          TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
+          TOTEM_TRY(totem::launch_plain_mul(ps, prop.as<float2>(), (int)vol, items, stream));
+          *launches += 3;
+          const int ev_mid = event_of_slice[k + 1];
+          if (ev_mid >= 0) {
+            TOTEM_TRY(totem::launch_plain_detect(ps, mask_mid.as<float>(), aper_num, (int)vol, items,
+                                                 part_e + ev_mid * part_stride, nblk, stream));
+            ++*launches;
+          }
+          TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_INVERSE));
+          TOTEM_TRY(totem::launch_plain_scale(ps, 1.f / (float)vol, (long)items * vol, stream));
+          *launches += 2;
+        }
         TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
-        TOTEM_TRY(totem::launch_plain_mul(ps, prop.as<float2>(), (int)vol, items, stream));
-        *launches += 3;
-        const int ev_mid = event_of_slice[k + 1];
-        if (ev_mid >= 0) {
-          TOTEM_TRY(totem::launch_plain_detect(ps, mask_mid.as<float>(), aper_num, (int)vol, items,
-                                               part_e + ev_mid * part_stride, nblk, stream));
-          ++*launches;
-        }
-        TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_INVERSE));
-        TOTEM_TRY(totem::launch_plain_scale(ps, 1.f / (float)vol, (long)items * vol, stream));
+        TOTEM_TRY(totem::launch_plain_detect(ps, mask_exit.as<float>(), aper_num, (int)vol, items,
+                                             part_e + exit_event * part_stride, nblk, stream));
         *launches += 2;
       }
-      TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
-      TOTEM_TRY(totem::launch_plain_detect(ps, mask_exit.as<float>(), aper_num, (int)vol, items,
-                                           part_e + exit_event * part_stride, nblk, stream));
-      *launches += 2;
+      for (int e = 0; e < n_events; ++e) {
+        TOTEM_TRY(totem::launch_det_reduce(part_e + e * part_stride, nblk, aper_num, items, (int)item0, depth,
+                                           acc.as<double>() + (size_t)e * w_num * ad, stream));
+        ++*launches;
+      }
     }
-    for (int e = 0; e < n_events; ++e) {
-      TOTEM_TRY(totem::launch_det_reduce(part_e + e * part_stride, nblk, aper_num, items, (int)item0, depth,
-                                         acc.as<double>() + (size_t)e * w_num * ad, stream));
-      ++*launches;
-    }
+    return combine_results(de, launches);
+  };
+
+  if (!fused || profiling || !totem::slice_graphs_enabled()) {
+    TOTEM_TRY(enqueue());
+  } else {
+    // what the launches embed: sizes, buffer addresses and the detection events
+    std::vector<long long> key = {h, items_total, B, slices, col_variant, t_storage, n_events, exit_event, aper_num,
+                                  w_num, depth, nblk, L, p_h, p_w, begin_row, begin_col, step, width_red,
+                                  (long long)tslice_bytes};
+    for (const void* q : {(const void*)psi.p, (const void*)part.p, (const void*)acc.p, (const void*)probe.p,
+                          (const void*)prop.p, (const void*)tw_n.p, (const void*)mask_mid.p, (const void*)mask_exit.p,
+                          Tslices, (const void*)gfsf_d.p, (const void*)out_result.p, (const void*)out_mid.p})
+      key.push_back((long long)(uintptr_t)q);
+    key.insert(key.end(), event_of_slice.begin(), event_of_slice.end());
+    key.insert(key.end(), de.layer_event.begin(), de.layer_event.end());
+    TOTEM_TRY(run_graphed(key, enqueue, launches));
   }
-  TOTEM_TRY(combine_results(de, launches));
   has_result = true;
   return Status::Ok();
+}
+
+// A run whose launches repeat an earlier run's exactly (same key) is captured into a CUDA graph
+// the second time and replayed from then on: one launch call instead of two per slice and
+// batch, and no host launch gaps between the short kernels of small requests.  The first run
+// with a new key executes directly (it also sets every kernel's shared-memory limit, which is
+// not done during capture).  Streams that cannot be captured (the legacy default stream, or one
+// the caller is capturing already) run directly.
+Status totem_session::run_graphed(const std::vector<long long>& key, const std::function<Status()>& enqueue,
+                                  int* launches) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool capturable = stream != nullptr && stream != cudaStreamLegacy && stream != cudaStreamPerThread &&
+                          cudaStreamIsCapturing(stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+  if (!capturable) return enqueue();
+  if (graph_exec != nullptr && key == graph_key) {
+    TOTEM_CUDA(cudaGraphLaunch(graph_exec, stream));
+    *launches += graph_launches;
+    return Status::Ok();
+  }
+  if (key != graph_key) {  // first run of this shape
+    drop_graph();
+    graph_key = key;
+    return enqueue();
+  }
+  const int before = *launches;
+  TOTEM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  const Status st = enqueue();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(stream, &g);
+  if (!st.ok() || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    graph_key.clear();
+    return st.ok() ? totem::cuda_status(e, "cudaStreamEndCapture") : st;
+  }
+  cudaGraphExec_t x = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    graph_key.clear();
+    return totem::cuda_status(ei, "cudaGraphInstantiate");
+  }
+  graph_exec = x;
+  graph_launches = *launches - before;
+  TOTEM_CUDA(cudaGraphLaunch(graph_exec, stream));
+  return Status::Ok();
+}
+
+void totem_session::drop_graph() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  graph_exec = nullptr;
+  graph_launches = 0;
 }
 
 totem::DetectionEvents totem_session::detection_events() const {
@@ -1011,6 +1085,13 @@ int totem_set_tx_builder(int mode, size_t scratch_bytes) {
     return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "unknown transmission builder mode"));
   g_tx_mode.store(mode);
   g_tx_scratch.store(scratch_bytes);
+  g_last_error.clear();
+  return TOTEM_OK;
+}
+
+int totem_set_slice_graphs(int enable) {
+  if (enable != 0 && enable != 1) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "enable must be 0 or 1"));
+  g_slice_graphs.store(enable);
   g_last_error.clear();
   return TOTEM_OK;
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <functional>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -184,6 +185,10 @@ struct totem_session {
   bool has_result = false;
   int last_what = 0;
   std::map<totem::PlanKey, cufftHandle> plans;
+  // the fused slice loop of the last run, as a CUDA graph (run_graphed)
+  std::vector<long long> graph_key;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0;
 
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   TotemTiming timing{};
@@ -198,6 +203,7 @@ struct totem_session {
     // buffers first: pool-backed ones are freed in order on ``stream``, which must still exist
     for_each_buf([](totem::DevBuf& b) { b.release(); });
     for (auto& kv : plans) cufftDestroy(kv.second);
+    drop_graph();
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& e : pev) cudaEventDestroy(e);
@@ -272,6 +278,8 @@ struct totem_session {
   Status slice_loop(int path, int batch, int col_variant, int t_storage, int* launches, int* batch_used);
   // The transmission slices as the slice loop reads them (complex64, or bfloat16 pairs).
   Status transmission_for(int t_storage, const void** t, size_t* slice_bytes, int* launches);
+  Status run_graphed(const std::vector<long long>& key, const std::function<Status()>& enqueue, int* launches);
+  void drop_graph();
   Status hrtem(const TotemHrtemArgs* h, TotemHrtemOut* out);
   Status run(int what, const TotemRunOptions* opt);
   Status collect_timing();
