@@ -134,3 +134,11 @@ def test_golden_fixture(name):
     assert rel_l2(res, g["result"]) < 1e-12
     if len(g["mid"]):
         assert rel_l2(mid, g["mid"]) < 1e-12
+
+
+def test_focal_spread_steps_must_be_odd():
+    from totem_b200 import optics
+    with pytest.raises(ValueError):
+        optics.gaussian_focal_weights(2, 4.0, 0.0025, 1.0)
+    d, w = optics.gaussian_focal_weights(3, 4.0, 0.0025, 1.0)
+    assert len(w) == 3 and d > 0

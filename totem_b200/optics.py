@@ -268,6 +268,8 @@ def gaussian_focal_weights(mtotal: int, rms_nm: float, lam_nm: float, gmax: floa
 
     Returns ``(delta_nm, weights)``.  ``mtotal`` must be odd; ``mtotal == 1`` gives ``(0, [1])``.
     """
+    if mtotal < 1 or mtotal % 2 == 0:
+        raise ValueError("the number of focal-spread steps must be odd (Gaussian_focal's -M..M)")
     M = (mtotal - 1) // 2
     if M == 0:
         return 0.0, np.array([1.0])
