@@ -356,8 +356,8 @@ __global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, in
 // g & 1; the partner's spectrum comes through shared memory.  A fine row that no atom touched
 // (row_used == 0; most rows of a crystal, whose atoms sit on lattice rows) is zero and so is its
 // transform: the pair skips all work (from N = 256, where a pair never shares a warp with
-// another pair's warp-level barriers).  A pair that ran zeroes the second half of both its rows
-// and its flag; the first halves of all rows (where the column pass writes) are cleared in bulk
+// another pair's warp-level barriers).  A pair that ran zeroes the second half of both its rows;
+// the first halves of all rows (where the column pass writes) and the flags are cleared in bulk
 // before each batch.  (A 128-register bound: the forward transform of a 16-byte-per-point row
 // does not fit 96.)
 template <int N>
@@ -368,7 +368,7 @@ struct GridRowCfg {
 };
 template <int N>
 __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCfg<N>::MINB)
-    k_grid_rows(void* __restrict__ grid, unsigned* __restrict__ row_used, const float4* __restrict__ ax, int p_h,
+    k_grid_rows(void* __restrict__ grid, const unsigned* __restrict__ row_used, const float4* __restrict__ ax, int p_h,
                 const float2* __restrict__ tw) {
   constexpr int P = GridRowCfg<N>::P, T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   extern __shared__ float2 sh[];
@@ -379,8 +379,7 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   const long qy = pair % p_h, t = pair / p_h;                 // t = 2 job + ey
   const long row0 = ((t >> 1) * 4 + 2 * (t & 1)) * p_h + qy;  // plane (ey, 0), row qy
   // fine row 2 qy + ey of job t / 2
-  unsigned* flag = row_used + (t >> 1) * 2 * p_h + 2 * qy + (t & 1);
-  const bool live = N < 256 || *flag != 0u;
+  const bool live = N < 256 || row_used[(t >> 1) * 2 * p_h + 2 * qy + (t & 1)] != 0u;
   longlong2* src = static_cast<longlong2*>(grid) + (row0 + ex * p_h) * N;
   float2 v[P];
   if (live) {
@@ -394,8 +393,7 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   __syncthreads();  // every point of the CTA's rows is in registers before any is overwritten
   const RowLayout<N> L;
   if (live) {
-    // clear what the next batch's bulk clear leaves out: the second half of both rows, and the flag
-    if (j == 0 && ex == 0) *flag = 0u;
+    // clear what the next batch's bulk clear leaves out: the second half of both rows
 #pragma unroll
     for (int m = P / 2; m < P; ++m) src[j + m * T] = make_longlong2(0, 0);
     fft_regs<N, false>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
@@ -421,10 +419,13 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
 // segments, whole sectors; 168 KB of shared memory), shorter ones the default width.
 template <int N>
 using GridColCfg = ColCfg<N, 4, (N == 4096) ? 4 : 0>;
-// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).
+// Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).  Plane pl is
+// (job pl / 2, parity ey = pl % 2); its row q is fine row 2 q + ey, which is zero when no atom
+// touched it (row_used == 0: the row pass left the cleared zeros there), so it is not read.
 template <int N>
 __global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCfg<N>::MINB)
-    k_grid_cols(float2* __restrict__ data, int width, long pitch, long plane_stride, const float2* __restrict__ tw) {
+    k_grid_cols(float2* __restrict__ data, int width, long pitch, long plane_stride, const unsigned* __restrict__ row_used,
+                const float2* __restrict__ tw) {
   constexpr int P = GridColCfg<N>::P, T = GridColCfg<N>::T, G = GridColCfg<N>::G;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
@@ -434,10 +435,14 @@ __global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCf
   const long pl = blockIdx.x / nblk;
   const int cb = blockIdx.x - (int)pl * nblk;
   float2* p = data + pl * plane_stride + cb * G + g;
+  const unsigned* used = row_used + (pl >> 1) * 2 * N + (pl & 1);  // row q: used[2 q]
   load_twiddles<N>(s_tw, tw);
   float2 v[P];
 #pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = p[(long)(j + m * T) * pitch];
+  for (int m = 0; m < P; ++m) {
+    const int q = j + m * T;
+    v[m] = __ldg(used + 2 * q) ? p[(long)q * pitch] : make_float2(0.f, 0.f);
+  }
   __syncthreads();
   fft_regs<N, false>(v, j, g, s_tw, s_x, ColLayout<N, G>(), SyncBlock());
 #pragma unroll
@@ -482,7 +487,7 @@ __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, S
 }
 
 template <int N>
-Status grid_rows(void* grid, unsigned* row_used, long pairs, const float2* ax, int p_h, const float2* tw,
+Status grid_rows(void* grid, const unsigned* row_used, long pairs, const float2* ax, int p_h, const float2* tw,
                  cudaStream_t st) {
   constexpr int T = GridRowCfg<N>::T, G = GridRowCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
@@ -494,13 +499,14 @@ Status grid_rows(void* grid, unsigned* row_used, long pairs, const float2* ax, i
 }
 
 template <int N>
-Status grid_cols(float2* data, long planes, int width, long pitch, long plane_stride, const float2* tw,
-                 cudaStream_t st) {
+Status grid_cols(float2* data, long planes, int width, long pitch, long plane_stride, const unsigned* row_used,
+                 const float2* tw, cudaStream_t st) {
   constexpr int T = GridColCfg<N>::T, G = GridColCfg<N>::G;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_grid_cols<N>, smem));
   if (width % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "grid width not a multiple of the column tile");
-  k_grid_cols<N><<<(unsigned)(planes * (width / G)), G * T, smem, st>>>(data, width, pitch, plane_stride, tw);
+  k_grid_cols<N><<<(unsigned)(planes * (width / G)), G * T, smem, st>>>(data, width, pitch, plane_stride, row_used,
+                                                                          tw);
   return cuda_status(cudaGetLastError(), "k_grid_cols");
 }
 
@@ -666,15 +672,16 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
   const long pitch = 2L * g.p_w, pstride = (long)g.p_h * pitch;
   const size_t plane_bytes = (size_t)plane * 64;  // four planes of 16-byte points per job
   unsigned* used = reinterpret_cast<unsigned*>(static_cast<char*>(scratch) + plane_bytes * per_batch);
-  // Between batches the kernels leave the second half of every fine row and the row flags zero;
-  // new scratch is cleared whole once, and the first halves (dense after the column pass) are
-  // cleared in bulk before each batch (a strided memset; clearing them in the combine after
-  // reading was measured 7x slower than the combine itself).
+  // Between batches the kernels leave the second half of every fine row zero; new scratch is
+  // cleared whole once, and the first halves (dense after the column pass) and the row flags are
+  // cleared in bulk before each batch (a strided memset; clearing the first halves in the combine
+  // after reading was measured 7x slower than the combine itself).
   if (!scratch_zero) TOTEM_CUDA(cudaMemsetAsync(scratch, 0, job_bytes * per_batch, st));
   for (const GridBatch& b : grid_batches(job_beg, per_batch)) {
     const int nj = b.j_hi - b.j_lo;
     if (nj > 0) {
       TOTEM_CUDA(cudaMemset2DAsync(scratch, 16 * (size_t)g.p_w, 0, 8 * (size_t)g.p_w, 4 * (size_t)g.p_h * nj, st));
+      TOTEM_CUDA(cudaMemsetAsync(used, 0, sizeof(unsigned) * 2 * g.p_h * nj, st));
       int most = 0;
       for (int j = b.j_lo; j < b.j_hi; ++j) most = std::max(most, jobs[j].w - jobs[j].z);
       const unsigned bx = (unsigned)std::min<long>(((long)most * GR_W + 255) / 256 + 1, 4096);
@@ -693,13 +700,13 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
         case 4096: TOTEM_TRY(grid_rows<4096>(scratch, used, pairs, gp.ax, g.p_h, tw_w, st)); break;
       }
       switch (g.p_h) {
-        case 64: TOTEM_TRY(grid_cols<64>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
-        case 128: TOTEM_TRY(grid_cols<128>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
-        case 256: TOTEM_TRY(grid_cols<256>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
-        case 512: TOTEM_TRY(grid_cols<512>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
-        case 1024: TOTEM_TRY(grid_cols<1024>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
-        case 2048: TOTEM_TRY(grid_cols<2048>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
-        case 4096: TOTEM_TRY(grid_cols<4096>(f, planes, g.p_w, pitch, 2 * pstride, tw_h, st)); break;
+        case 64: TOTEM_TRY(grid_cols<64>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
+        case 128: TOTEM_TRY(grid_cols<128>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
+        case 256: TOTEM_TRY(grid_cols<256>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
+        case 512: TOTEM_TRY(grid_cols<512>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
+        case 1024: TOTEM_TRY(grid_cols<1024>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
+        case 2048: TOTEM_TRY(grid_cols<2048>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
+        case 4096: TOTEM_TRY(grid_cols<4096>(f, planes, g.p_w, pitch, 2 * pstride, used, tw_h, st)); break;
       }
       *launches += 3;
     }
