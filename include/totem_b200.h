@@ -359,7 +359,7 @@ typedef struct TotemServerOptions {
   int ticks_ahead;               /* slice steps queued ahead of the GPU; 0 = 4                 */
   int policy;                    /* TOTEM_SCHED_*                                              */
   int prep_threads;              /* host threads preparing requests (upload, transmission);
-                                    0 = 1                                                      */
+                                    0 = 2                                                      */
 } TotemServerOptions;
 
 enum {

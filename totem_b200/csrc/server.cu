@@ -620,9 +620,11 @@ int totem_server_create(const TotemServerOptions* opt, totem_server** out) {
     return server_fail(st);
   }
   totem_server* raw = s.get();
-  // one preparation thread by default: concurrent uploads from pageable memory were measured to
-  // contend (mean preparation 16-31 ms per request with one thread, 52-177 ms with three)
-  const int np = o.prep_threads > 0 ? o.prep_threads : 1;
+  // two preparation threads by default: with a mix up to 1024^2 windows (2048^2 potentials)
+  // burst throughput was 218-221K probe*slices/s against 202-209K with one, and equal within
+  // the run-to-run spread on 256^2/512^2 mixes; three were slower (concurrent uploads from
+  // pageable memory contend: 52-177 ms per preparation against 16-31 ms with one thread)
+  const int np = o.prep_threads > 0 ? o.prep_threads : 2;
   raw->prep_live = np;
   for (int i = 0; i < np; ++i) raw->prep_thrs.emplace_back(run_worker, raw, 0);
   raw->sched_thr = std::thread(run_worker, raw, 1);
