@@ -439,9 +439,11 @@ struct RowCfg {
   static constexpr int G = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
   // resident CTAs of 128 threads requested per SM: 5 caps registers at 96 per thread, which
   // the padded exchange addressing fits without spilling up to N = 1024 (and 5 CTAs is also
-  // what the row pass's shared memory allows); from N = 2048 (three-stage transforms) 3, i.e.
-  // ~170 registers: the 2048 row pass spilled 200 B at 128 and ran 22 % slower
-  static constexpr int CTAS128 = (N <= 1024) ? 5 : 3;
+  // what the row pass's shared memory allows).  At 1024 a 128-register cap (4 CTAs) made the
+  // row pass 12 % faster (3.51 against 4.01 us per probe; no change at 512); from N = 2048
+  // (three-stage transforms) 3, i.e. ~170 registers: the 2048 row pass spilled 200 B at 128
+  // and ran 22 % slower
+  static constexpr int CTAS128 = (N <= 512) ? 5 : (N <= 1024 ? 4 : 3);
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };
 // Columns: G adjacent columns per CTA, thread (j, g) = (tid / G, tid % G), so a warp's loads
