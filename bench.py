@@ -203,6 +203,68 @@ def run_reference(ns):
     print(json.dumps(line), flush=True)
 
 
+def _event_seconds(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1000.0
+
+
+def plain_comparators(ns, req, local, stream, fused_value):
+    """The metric's comparator: the plain cuFFT path (cuFFT plus one element-wise kernel per step)
+    on the same GPU, (a) batched over the whole request (1 GiB of waves per batch) and (b) one
+    probe at a time, the reference's loop structure (cuda_source_lobato.cu:1313-1398 runs one
+    cuFFT plan over the probes of a batch; ToTem's CPU path and small batches go probe by probe),
+    on a sample of 8x8 probes of the same workload (same window, potential and slices: the
+    per-probe cost does not depend on the raster)."""
+    from totem_b200 import capi
+    s = capi.Session(device=local, stream=stream.cuda_stream)
+    s.upload(req)
+    s.run(path=capi.PATH_PLAIN)  # cuFFT plans, transmission
+    t_batched = _event_seconds(stream, lambda: s.run(path=capi.PATH_PLAIN))
+    batch_plain = s.timing().batch
+    s.close()
+    sub = build_workload(ns.workload, raster=8)
+    s = capi.Session(device=local, stream=stream.cuda_stream)
+    s.upload(sub)
+    s.run(path=capi.PATH_PLAIN, batch=1)
+    t_probe = _event_seconds(stream, lambda: s.run(path=capi.PATH_PLAIN, batch=1, skip_transmission=True))
+    s.close()
+    batched = req.probe_slices / t_batched
+    per_probe = sub.probe_slices / t_probe
+    return {
+        "batched": {"value": batched, "unit": "probe*slices/s", "batch": batch_plain,
+                    "what": "whole request (transmission + slice loop), same workload, CUDA events"},
+        "per_probe": {"value": per_probe, "unit": "probe*slices/s", "batch": 1,
+                      "what": f"slice loop of {sub.depth} probes of the same workload, one probe per cuFFT plan "
+                              "execution, transmission built beforehand"},
+        "fused_vs_batched": fused_value / batched, "fused_vs_per_probe": fused_value / per_probe,
+    }
+
+
+def serving_leg(local):
+    """Latency under load: a seeded mix of STEM requests (windows 256^2 / 512^2, probes
+    log-uniform 1-256, 20-100 slices, Peng / Lobato) through the continuous-batching server,
+    first all at once (capacity), then with seeded Poisson arrivals at 85 % of that capacity."""
+    from totem_b200 import serving
+    reqs = serving.make_workload(count=32, seed=0, sizes=(256, 512), max_probes=256, slices=(20, 100))
+    serving.serve(reqs[:4], np.zeros(4), device=local)  # kernels, pools
+    _, lat_b, mk_b = serving.serve(reqs, np.zeros(len(reqs)), device=local)
+    rate = 0.85 * len(reqs) / mk_b
+    _, lat_p, mk_p = serving.serve(reqs, serving.poisson_arrivals(len(reqs), rate, 0), device=local)
+    ps = sum(r.probe_slices for r in reqs)
+    return {"workload": "32 seeded requests, windows 256^2/512^2, probes log-uniform 1-256, slices 20-100, "
+                        "Peng/Lobato, SrTiO3 filling the potential grid",
+            "burst": {"probe_slices_per_s": ps / mk_b, "p50_ms": float(np.percentile(lat_b, 50)),
+                      "p99_ms": float(np.percentile(lat_b, 99))},
+            "poisson": {"rate_hz": rate, "probe_slices_per_s": ps / mk_p, "p50_ms": float(np.percentile(lat_p, 50)),
+                        "p99_ms": float(np.percentile(lat_p, 99))}}
+
+
 def workload_config(ns, req):
     return {"workload": f"{ns.workload}: SrTiO3 [001] STEM-ADF, {req.depth} probes x {req.slices} slices, "
                         f"window {req.height}^2, potential {req.p_height}^2, Peng, 300 kV",
@@ -226,6 +288,7 @@ def main():
     ap.add_argument("--col-variant", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-comparators", action="store_true", help="skip the plain cuFFT and serving legs")
     ns = ap.parse_args()
     if ns.impl == "reference":
         run_reference(ns)
@@ -326,6 +389,11 @@ def main():
         e2e = {"value": ws * units * ns.steps / dt, "unit": "probe*slices/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "api": "totem_stem_run (host buffers)"}
 
+    plain = serve = None
+    if rank == 0 and ws == 1 and not ns.no_comparators and path == capi.PATH_FUSED:
+        plain = plain_comparators(ns, req, local, stream, value)
+        serve = serving_leg(local)
+
     cpu = None
     if rank == 0 and ws == 1 and not ns.no_cpu_baseline:
         from oracle import stem_oracle as so
@@ -341,8 +409,11 @@ def main():
             "data": "synthetic (seeded SrTiO3 supercell, random-free probe)",
             "config": workload_config(ns, req), "batch": batch_used,
             "gpu_launches": launches * ns.steps, "clocks": clk.summary(), "roofline": roofline,
-            "e2e": e2e, "cpu_baseline": cpu,
+            "e2e": e2e, "cpu_baseline": cpu, "plain_cufft": plain, "serving": serve,
         }
+        if serve:
+            line["latency"] = {"p50_ms": serve["poisson"]["p50_ms"], "p99_ms": serve["poisson"]["p99_ms"],
+                               "what": "serving leg, Poisson arrivals at 85 % of capacity"}
         print(json.dumps(line), flush=True)
     sess.close()
     if dist:

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define TOTEM_ABI_VERSION 2
+#define TOTEM_ABI_VERSION 3
 
 /* Status codes.  The reference returns silently or aborts MATLAB (waveCuda.cpp:7-16,
  * cuda_source_lobato.cu:1253-1256); every entry point here returns one of these instead. */
@@ -57,9 +57,13 @@ enum {
 enum { TOTEM_PARAM_PENG = 0,   /* rows of 13 (neutral) / 25 (ionic) columns */
        TOTEM_PARAM_LOBATO = 1  /* rows of 14 / 26 columns                     */ };
 
-/* Slice-loop implementation. */
-enum { TOTEM_PATH_FUSED = 0,   /* shared-memory FFT passes fused with the multiplies and detectors */
-       TOTEM_PATH_PLAIN = 1    /* cuFFT plus separate element-wise kernels (comparator)           */ };
+/* Slice-loop implementation.  TOTEM_PATH_FUSED runs the hand-written kernels where they apply
+ * (square power-of-two windows of 64..2048 for the slice loop, power-of-two potential grids of
+ * 64..4096 for the transmission FFT) and cuFFT elsewhere; TotemTiming reports what ran.
+ * TOTEM_PATH_FUSED_ONLY fails with TOTEM_ERR_UNSUPPORTED instead of using cuFFT. */
+enum { TOTEM_PATH_FUSED = 0,      /* shared-memory FFT passes fused with the multiplies and detectors */
+       TOTEM_PATH_PLAIN = 1,      /* cuFFT plus separate element-wise kernels (comparator)           */
+       TOTEM_PATH_FUSED_ONLY = 2  /* the fused kernels or an error, never cuFFT                     */ };
 
 /*
  * The inputs of myProjectfun (waveCuda.h:10-21), one field per parameter, same meaning.
@@ -139,6 +143,10 @@ typedef struct TotemTiming {
   int row_pass_launches, col_pass_launches;
   long long probe_slices;          /* probes x slices advanced by the run                      */
   long long h2d_bytes, d2h_bytes;  /* host<->device bytes of the last upload / download        */
+  /* what ran (-1 = that stage did not run): */
+  int slice_path;                  /* TOTEM_PATH_FUSED or TOTEM_PATH_PLAIN (cuFFT)               */
+  int tx_fft_path;                 /* transmission inverse FFT: TOTEM_PATH_FUSED or _PLAIN (cuFFT) */
+  int tx_builder;                  /* TOTEM_TX_DIRECT, TOTEM_TX_GRIDDING or TOTEM_TX_ROWS          */
 } TotemTiming;
 
 typedef struct totem_session totem_session;
@@ -185,6 +193,9 @@ TOTEM_API int totem_transmission_run(const TotemStemArgs *args, TotemStemOut *ou
 #define TOTEM_TX_AUTO 0
 #define TOTEM_TX_DIRECT 1
 #define TOTEM_TX_GRIDDING 2
+/* Reported in TotemTiming.tx_builder only: one thread per pixel and atom row (reciprocal grids
+ * that are not the separable meshgrid). */
+#define TOTEM_TX_ROWS 3
 TOTEM_API int totem_set_tx_builder(int mode, size_t scratch_bytes);
 /* Repeated runs of a session's fused slice loop with the same shapes and buffers replay as one
  * CUDA graph (captured on the second such run): 1 = on (default), 0 = off.  Process-wide; no
@@ -254,9 +265,13 @@ TOTEM_API int totem_frozen_phonon(const double *table, int n, int ncol, double e
  * needs more (about 15 probes of 512^2 per call) fails with TOTEM_ERR_INVALID_ARG and a message
  * (totem_last_error) giving the largest batch that fits.  The first call on a device performs a
  * one-time set-up with that device current (the array's device address and a blocking copy of
- * FFT twiddle tables into it); make that first call before any stream capture.  Every call
- * shares the array: calls that overlap on the GPU race; calls ordered on one stream do not.
- * n must be a power of two in [64, 2048] and slices >= 1.  Asynchronous on ``stream``.
+ * FFT twiddle tables into it); make that first call before any stream capture.  The set-up
+ * belongs to the device's current CUDA context and is repeated when another context becomes
+ * current (after cudaDeviceReset, or under a caller's own driver-API context), so the first call
+ * after such a change must also come before any capture.  Every call shares the array: calls that
+ * overlap on the GPU race; calls ordered on one stream do not.  n must be a power of two in
+ * [64, 1024] (a single 2048^2 probe would need the whole array) and slices >= 1.  Asynchronous on
+ * ``stream``.
  */
 TOTEM_API int totem_stem_slices_noalloc(const void *transmission, int p_height, int p_width, int slices,
                                         const void *probe, int w_num, const void *propagator, const float *masks,
@@ -342,7 +357,9 @@ TOTEM_API int totem_tcc_stack(const TotemAberrations *ab, double lambda_nm, int 
 typedef struct totem_server totem_server;
 
 enum {
-  TOTEM_SCHED_FIFO = 0,          /* wave memory goes to requests in arrival order              */
+  TOTEM_SCHED_FIFO = 0,          /* wave memory goes to prepared requests in arrival (ticket)
+                                    order; one still being prepared does not hold back a later
+                                    one that is ready                                          */
   TOTEM_SCHED_SHORTEST = 1       /* ... to the request with the least remaining work first, and
                                     preparation takes the cheapest queued request first         */
 };

@@ -72,7 +72,7 @@ def test_status_strings(lib):
         s = lib.totem_status_string(code).decode()
         assert s and s != "unknown status"
     assert lib.totem_status_string(99).decode() == "unknown status"
-    assert lib.totem_abi_version() == 2
+    assert lib.totem_abi_version() == 3
 
 
 def _has_gpu():
@@ -113,3 +113,13 @@ def test_slice_graph_switch_is_validated(lib):
     assert lib.totem_set_slice_graphs(2) == capi.ERR_INVALID_ARG
     assert lib.totem_set_slice_graphs(0) == capi.OK
     assert lib.totem_set_slice_graphs(1) == capi.OK
+
+
+def test_noalloc_rejects_2048_windows_before_any_device_call(lib):
+    # one 2048^2 probe would need the whole fixed scratch array: refused while validating the
+    # arguments, before the entry point touches a device (so this runs without a GPU)
+    fake = C.c_void_p(256)
+    rc = lib.totem_stem_slices_noalloc(fake, 4096, 4096, 2, fake, 1, fake, fake, 2, 2048, 8, 0, 0, 1, 1, 0, 1,
+                                       fake, None)
+    assert rc == capi.ERR_UNSUPPORTED
+    assert "1024" in lib.totem_last_error().decode()

@@ -150,3 +150,32 @@ def test_invalid_window_rejected(engine_lib):
     with pytest.raises(capi.TotemError) as e:
         capi.stem_run(bad)
     assert e.value.code == capi.ERR_INVALID_ARG
+
+
+def test_path_used_is_reported_and_fused_only_refuses_cufft(engine_lib):
+    # a 96^2 window on a 160^2 grid: no hand-written transform of these lengths, so the fused
+    # request runs on cuFFT, says so in its timing, and TOTEM_PATH_FUSED_ONLY refuses it
+    odd = request.build_small_stem(n=96, p=160, raster=(2, 2), step=5, slices=3, mid_layer=(2,))
+    s = capi.Session()
+    s.upload(odd)
+    s.run(path=capi.PATH_FUSED)
+    res, mid, _ = s.download()
+    t = s.timing()
+    assert (t.slice_path, t.tx_fft_path) == (capi.PATH_PLAIN, capi.PATH_PLAIN)
+    assert t.tx_builder in (capi.TX_DIRECT, capi.TX_GRIDDING)
+    _check(odd, res, mid)
+    with pytest.raises(capi.TotemError) as e:
+        s.run(path=capi.PATH_FUSED_ONLY)
+    assert e.value.code == capi.ERR_UNSUPPORTED and "FUSED_ONLY" in str(e.value)
+    s.close()
+    ok = request.build_small_stem()
+    s = capi.Session()
+    s.upload(ok)
+    s.run(path=capi.PATH_FUSED_ONLY)
+    res, mid, _ = s.download()
+    t = s.timing()
+    assert (t.slice_path, t.tx_fft_path) == (capi.PATH_FUSED, capi.PATH_FUSED)
+    _check(ok, res, mid)
+    s.run(path=capi.PATH_PLAIN)
+    assert s.timing().slice_path == capi.PATH_PLAIN
+    s.close()

@@ -37,12 +37,40 @@ def _worker(rank, world, port, what, out_dir):
         if what == "bands":
             req = request.build_small_stem(raster=(5, 3), slices=3, mid_layer=(2,))
             res, mid = shard.stem_sharded(req, compute=_oracle_compute)
+        elif what == "pinning":
+            # the default compute: a session on this rank's GPU (LOCAL_RANK), with the engine's
+            # session replaced by a recorder so that no device is needed
+            os.environ["LOCAL_RANK"] = str(rank)
+            from totem_b200 import capi
+            capi.Session = _RecordingSession
+            req = request.build_small_stem(raster=(4, 3), slices=2, mid_layer=())
+            res, mid = shard.stem_sharded(req)
+            res = np.asarray(_RecordingSession.devices, dtype=float)
         else:
             confs = shard.PhononConfigurations(partial(_small_phonon), 3)
             res, mid = shard.configurations_summed(confs, compute=_oracle_compute)
         np.savez(os.path.join(out_dir, f"r{rank}.npz"), res=res, mid=mid)
     finally:
         dist.destroy_process_group()
+
+
+class _RecordingSession:
+    """Stands in for ``capi.Session``: records the device each session was opened on and returns
+    zero images of the right size."""
+    devices = []
+
+    def __init__(self, device=-1, stream=None):
+        _RecordingSession.devices.append(device)
+
+    def upload(self, req, stem=True):
+        self.req = req
+
+    def run(self, **kw):
+        pass
+
+    def download(self, want_transmission=False):
+        r = self.req
+        return np.zeros(r.aper_num * r.depth), np.zeros(r.aper_num * r.depth * len(r.mid_layer)), None
 
 
 def _small_phonon(phonon_seed):
@@ -89,3 +117,17 @@ def test_phonon_configurations_summed_over_ranks(tmp_path):
     ref_mid = sum(r[1] for r in ref)
     for o in outs:
         assert np.allclose(o["res"], ref_res, rtol=1e-13) and np.allclose(o["mid"], ref_mid, rtol=1e-13)
+
+
+@pytest.mark.timeout(600)
+def test_sharded_default_compute_pins_the_rank_gpu(tmp_path):
+    outs = _run("pinning", tmp_path)
+    # each rank opened exactly one session, on the GPU of its LOCAL_RANK
+    assert [list(o["res"]) for o in outs] == [[0.0], [1.0]]
+
+
+def test_local_device_reads_local_rank(monkeypatch):
+    monkeypatch.setenv("LOCAL_RANK", "3")
+    assert shard.local_device() == 3
+    monkeypatch.delenv("LOCAL_RANK")
+    assert shard.local_device() == -1

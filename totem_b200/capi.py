@@ -22,7 +22,7 @@ OK, ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_CUFFT, ERR_OOM, ERR_NO_DEVIC
 SCHED_FIFO, SCHED_SHORTEST = 0, 1
 REQ_QUEUED, REQ_PREPARING, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
 PARAM_PENG, PARAM_LOBATO = 0, 1
-PATH_FUSED, PATH_PLAIN = 0, 1
+PATH_FUSED, PATH_PLAIN, PATH_FUSED_ONLY = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -71,7 +71,8 @@ class TotemTiming(C.Structure):
                 ("kernel_launches", C.c_int), ("batch", C.c_int),
                 ("row_pass_ms", C.c_float), ("col_pass_ms", C.c_float),
                 ("row_pass_launches", C.c_int), ("col_pass_launches", C.c_int),
-                ("probe_slices", C.c_longlong), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong)]
+                ("probe_slices", C.c_longlong), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong),
+                ("slice_path", C.c_int), ("tx_fft_path", C.c_int), ("tx_builder", C.c_int)]
 
 
 class TotemServerOptions(C.Structure):
@@ -537,7 +538,7 @@ def frozen_phonon(table, eachthick: float, slicethick, seed: int) -> np.ndarray:
     return out
 
 
-TX_AUTO, TX_DIRECT, TX_GRIDDING = 0, 1, 2
+TX_AUTO, TX_DIRECT, TX_GRIDDING, TX_ROWS = 0, 1, 2, 3
 
 
 def set_slice_graphs(enable: bool):

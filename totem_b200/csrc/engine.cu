@@ -336,6 +336,10 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
 // ---------------------------------------------------------------------------------------------
 Status totem_session::build_transmission(int path, int* launches) {
   const size_t plane = (size_t)p_h * p_w;
+  const bool fft_fused = totem::fused_fft_size_ok(p_h) && totem::fused_fft_size_ok(p_w);
+  if (path == TOTEM_PATH_FUSED_ONLY && !fft_fused && slices > 0)
+    return Status::Err(TOTEM_ERR_UNSUPPORTED,
+                       "TOTEM_PATH_FUSED_ONLY: the transmission FFT needs a power-of-two potential grid of 64..4096");
   TOTEM_TRY(T.ensure(plane * std::max(slices, 1) * sizeof(float2)));
   if (slices == 0) return Status::Ok();
   totem::TxGrid g;
@@ -371,6 +375,7 @@ Status totem_session::build_transmission(int path, int* launches) {
       gp.jobs = grid_jobs.as<int4>(); gp.job_beg = grid_job_beg.as<int>();
       const bool was_zero = grid_scratch_zero;
       grid_scratch_zero = false;  // until every batch has been enqueued
+      ran_tx_builder = TOTEM_TX_GRIDDING;
       TOTEM_TRY(totem::launch_tx_gridding(g, sn, si, gp, grid_job_beg_h, grid_jobs_h, tw_pw.as<float2>(),
                                           tw_ph.as<float2>(), grid_scratch.p, bytes, was_zero, T.as<float2>(), stream,
                                           launches));
@@ -382,6 +387,7 @@ Status totem_session::build_transmission(int path, int* launches) {
         grid_scratch_zero = false;
       }
     } else {
+      ran_tx_builder = TOTEM_TX_DIRECT;
       TOTEM_TRY(totem::launch_tx_species(g, sn, si, T.as<float2>(), stream));
       ++*launches;
     }
@@ -393,15 +399,18 @@ Status totem_session::build_transmission(int path, int* launches) {
   } else {
     const auto vn = rows_n.view(n_rows > 0, has_abs_n, ncoef_n);
     const auto vi = rows_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
+    ran_tx_builder = TOTEM_TX_ROWS;
     TOTEM_TRY(totem::launch_tx_structure(g, vn, vi, vcn, vci, T.as<float2>(), stream));
     ++*launches;
   }
   const float sig = (float)(sigma / 1000.0);
-  if (path == TOTEM_PATH_FUSED && totem::fused_fft_size_ok(p_h) && totem::fused_fft_size_ok(p_w)) {
+  if (path != TOTEM_PATH_PLAIN && fft_fused) {
+    ran_tx_fft = TOTEM_PATH_FUSED;
     TOTEM_TRY(totem::launch_tx_fft_exp(T.as<float2>(), slices, p_h, p_w, sig, tw_pw.as<float2>(),
                                        tw_ph.as<float2>(), stream));
     *launches += 2;
   } else {
+    ran_tx_fft = TOTEM_PATH_PLAIN;
     cufftHandle p;
     TOTEM_TRY(plan(p_h, p_w, slices, &p));
     TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)T.p, (cufftComplex*)T.p, CUFFT_INVERSE));
@@ -509,7 +518,11 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   const std::vector<int>& event_of_slice = de.event_of_slice;
   const int n_events = de.n_events, exit_event = de.exit_event;
 
-  const bool fused = (path == TOTEM_PATH_FUSED) && h == w && is_pow2(h) && h >= 64 && h <= 2048 && slices > 0;
+  const bool fused = (path != TOTEM_PATH_PLAIN) && h == w && is_pow2(h) && h >= 64 && h <= 2048 && slices > 0;
+  if (path == TOTEM_PATH_FUSED_ONLY && !fused && slices > 0)
+    return Status::Err(TOTEM_ERR_UNSUPPORTED,
+                       "TOTEM_PATH_FUSED_ONLY: the fused slice loop needs a square power-of-two window of 64..2048");
+  ran_slice_path = fused ? TOTEM_PATH_FUSED : TOTEM_PATH_PLAIN;
   const size_t vol = (size_t)h * w;
   int B = batch;
   if (B <= 0) {
@@ -808,7 +821,7 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
   if (!uploaded) return Status::Err(TOTEM_ERR_STATE, "run before a successful upload");
   TotemRunOptions o{};
   if (opt) o = *opt;
-  if (o.path != TOTEM_PATH_FUSED && o.path != TOTEM_PATH_PLAIN)
+  if (o.path != TOTEM_PATH_FUSED && o.path != TOTEM_PATH_PLAIN && o.path != TOTEM_PATH_FUSED_ONLY)
     return Status::Err(TOTEM_ERR_INVALID_ARG, "unknown path");
   TOTEM_CUDA(cudaSetDevice(device));
   for (auto& e : ev)
@@ -816,6 +829,7 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
   int launches = 0, batch_used = 0;
   has_result = false;
   last_what = what;
+  ran_slice_path = ran_tx_fft = ran_tx_builder = -1;
   profiling = o.profile != 0;
   pkind.clear();
   pused = 0;
@@ -836,6 +850,9 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
   timing.batch = batch_used;
   timing.probe_slices = (what == 0) ? (long long)w_num * depth * slices : 0;
   timing.h2d_bytes = h2d_bytes;
+  timing.slice_path = ran_slice_path;
+  timing.tx_fft_path = ran_tx_fft;
+  timing.tx_builder = ran_tx_builder;
   timing_pending = true;
   return Status::Ok();
 }

@@ -14,11 +14,16 @@
 //    library, for the life of the process;
 //  * the first call on a device does a one-time set-up with that device current: it looks up
 //    the array's device address (cudaGetSymbolAddress) and copies the FFT twiddle tables into it
-//    with a blocking copy.  Make that first call before any stream capture;
+//    with a blocking copy.  Make that first call before any stream capture.  The set-up belongs
+//    to the device's current CUDA context: it is done again when another context becomes
+//    current on that device (after cudaDeviceReset, or a caller's own driver-API context);
+//  * windows of 64^2 .. 1024^2: one 2048^2 probe alone (32 MiB) would fill the whole array;
 //  * every call uses the same array and leaves its contents behind; two calls that overlap on
 //    the GPU (different streams, or different host threads without ordering) race on it.
 //    Everything a call reads from the array it has written itself first in stream order, so
 //    back-to-back calls on one stream are independent.
+#include <cuda.h>  // driver-API types of the two context queries looked up through the runtime
+
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -29,7 +34,8 @@
 namespace {
 
 constexpr size_t NOALLOC_SCRATCH_BYTES = 32ull << 20;  // 32 MiB per GPU
-constexpr size_t NOALLOC_TW_BYTES = 64u << 10;         // twiddle tables of N = 64 .. 2048
+constexpr size_t NOALLOC_TW_BYTES = 64u << 10;         // twiddle tables of N = 64 .. 1024
+constexpr int NOALLOC_MAX_N = 1024;
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
@@ -37,11 +43,39 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 struct DeviceScratch {
   unsigned char* base = nullptr;  // device address of g_noalloc_scratch on that device
   size_t tw_offset[12] = {};      // byte offset of the twiddle table of N = 2^k
+  unsigned long long context = 0; // id of the context the address and the tables belong to
 };
 
 std::mutex g_setup_mu;
 DeviceScratch g_dev[NOALLOC_MAX_DEVICES];
 bool g_ready[NOALLOC_MAX_DEVICES] = {};
+
+// Id of the calling thread's current CUDA context, unique for the life of the process
+// (cuCtxGetId), or 0 when no context is current.  The two driver functions are looked up through
+// the runtime once, so the library keeps no link-time dependency on the driver library.
+unsigned long long current_context_id() {
+  using GetCurrentFn = CUresult (*)(CUcontext*);
+  using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    void* f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(f);
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c != nullptr && get_id(c, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
 
 int log2i(int n) {
   int k = 0;
@@ -49,17 +83,21 @@ int log2i(int n) {
   return k;
 }
 
-// One-time set-up on the current device: device address of the array, twiddle tables.
+// Set-up on the current device, once per device and context: device address of the array,
+// twiddle tables.
 totem::Status setup(int dev, DeviceScratch** out) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return totem::Status::Err(TOTEM_ERR_UNSUPPORTED, "device index too large");
-  if (!g_ready[dev]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_ready[dev] || ctx == 0 || ctx != g_dev[dev].context) {
+    g_ready[dev] = false;
     DeviceScratch d;
     void* p = nullptr;
-    TOTEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    TOTEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));  // makes the device's context current
     d.base = static_cast<unsigned char*>(p);
+    d.context = current_context_id();
     size_t off = 0;
-    for (int n = 64; n <= 2048; n *= 2) {
+    for (int n = 64; n <= NOALLOC_MAX_N; n *= 2) {
       const std::vector<float2> tw = totem::stage_twiddles(n);
       const size_t bytes = tw.size() * sizeof(float2);
       if (off + bytes > NOALLOC_TW_BYTES) return totem::Status::Err(TOTEM_ERR_UNSUPPORTED, "twiddle region too small");
@@ -80,8 +118,10 @@ totem::Status run(const void* transmission, int p_height, int p_width, int slice
   using totem::Status;
   if (!transmission || !probe || !propagator || !masks || !result)
     return Status::Err(TOTEM_ERR_INVALID_ARG, "NULL device pointer");
-  if (n < 64 || n > 2048 || (n & (n - 1)))
-    return Status::Err(TOTEM_ERR_UNSUPPORTED, "window edge must be a power of two in [64, 2048]");
+  if (n < 64 || n > NOALLOC_MAX_N || (n & (n - 1)))
+    return Status::Err(TOTEM_ERR_UNSUPPORTED,
+                       "window edge must be a power of two in [64, 1024] (one 2048^2 probe needs more than the "
+                       "fixed scratch array)");
   if (slices < 1) return Status::Err(TOTEM_ERR_INVALID_ARG, "slices must be >= 1");
   if (aper_num < 1 || aper_num > 32) return Status::Err(TOTEM_ERR_INVALID_ARG, "aper_num must be in [1, 32]");
   if (w_num < 1 || depth < 1 || width_red < 1 || step < 0 || items < 1 || item0 < 0 ||

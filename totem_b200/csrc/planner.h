@@ -46,8 +46,10 @@ class Planner {
   size_t inflight() const { return inflight_; }
   const std::vector<PlanGroup>& active() const { return active_; }
 
-  // Groups that start at ``tick``.  Requests are visited in arrival order (FIFO) or by least
-  // remaining work, probes x slices (SHORTEST).  Each may start up to chunk_bytes of probes per
+  // Groups that start at ``tick``.  Requests are visited in arrival order, i.e. by ticket (FIFO;
+  // with several preparation threads requests can become ready out of order, and a later one
+  // that is ready does not wait for an earlier one still being prepared), or by least remaining
+  // work, probes x slices (SHORTEST).  Each may start up to chunk_bytes of probes per
   // tick while the wave memory in flight stays within wave_bytes.  FIFO stops at the first
   // request that cannot start (no overtaking); SHORTEST lets smaller requests fill the gap.  A
   // single probe larger than wave_bytes starts alone when nothing else is in flight.
@@ -59,6 +61,8 @@ class Planner {
       std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
         return work(pending_[a]) < work(pending_[b]);
       });
+    else
+      std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return pending_[a].id < pending_[b].id; });
     for (size_t idx : order) {
       if (active_.size() + out.size() >= max_groups_) break;
       PlanRequest& r = pending_[idx];

@@ -75,4 +75,6 @@ def main(ref_dir: str) -> str:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python -m totem_b200.data.extract_tables <directory holding Lobato_para.m and ABSFpara.m>")
+    main(sys.argv[1])

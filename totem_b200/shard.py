@@ -10,7 +10,7 @@ frozen-phonon configurations.  Two ways to use several GPUs:
     summed locally and reduced once (``all_reduce``).
 
 ``compute(req) -> (result, mid)`` does one request on the local device; the default is the
-engine (``capi.stem_run``).  Collectives go through ``torch.distributed`` (NCCL on GPUs, gloo
+engine, through a session on the rank's own GPU (``LOCAL_RANK``).  Collectives go through ``torch.distributed`` (NCCL on GPUs, gloo
 on CPU) and are only used for the final gather / reduction.
 """
 from __future__ import annotations
@@ -38,9 +38,30 @@ def band_request(req, r0: int, r1: int):
     return replace(req, beginrow=req.beginrow + r0 * req.step, hight_red=r1 - r0)
 
 
+def local_device() -> int:
+    """This rank's GPU: ``LOCAL_RANK`` as set by ``torchrun`` (one process per GPU), or -1 outside
+    a launcher (the engine then picks the GPU with the most free memory)."""
+    import os
+    v = os.environ.get("LOCAL_RANK")
+    return int(v) if v not in (None, "") else -1
+
+
+_SESSIONS = {}
+
+
 def _default_compute(req):
+    """One request on this rank's own GPU through a session kept per device.  A session pinned to
+    ``LOCAL_RANK`` keeps ranks off each other's GPUs: the one-shot ``totem_stem_run`` would pick
+    the GPU with the most free memory, which several ranks can agree on."""
     from . import capi
-    return capi.stem_run(req)
+    dev = local_device()
+    s = _SESSIONS.get(dev)
+    if s is None:
+        s = _SESSIONS[dev] = capi.Session(device=dev)
+    s.upload(req)
+    s.run()
+    res, mid, _ = s.download()
+    return res, mid
 
 
 def stem_sharded(req, compute=None, group=None):
