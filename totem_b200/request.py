@@ -188,6 +188,29 @@ def build_srtio3_stem(cells=(8, 8, 50), n: int = 512, sampling: float = 0.0625, 
                          native_slicing=native_slicing)
 
 
+def build_stem_from_table(atoms, eachthick: float, slicethick, n: int = 128, p: int = 256, sampling: float = 0.15,
+                          step: int = 16, raster=(3, 3), flag: str = PENG, kv: float = 300.0,
+                          semi_angle: float = 25.0, c3_um: float = -5.0, defocus_nm: float = 0.0,
+                          detectors=((60.0, 200.0), (0.0, 10.0)), mid_layer=(), multiceng: int = 0,
+                          native_slicing: bool = False) -> StemRequest:
+    """A STEM request on a specimen given as ToTem's atom table (``allresul.x_new``: one row per
+    atom ``Z x y z valence ionic-fraction B occupancy``, Angstrom) with its slicing (``eachthick``
+    and the slice tops ``slicethick``, slicingdisplay.m:228-254), at the coordinates given (not
+    re-centred).  The scan is centred on the ``p`` x ``p`` potential grid."""
+    atoms = np.asarray(atoms, dtype=np.float64)
+    slicethick = np.asarray(slicethick, dtype=np.float64)
+    if not np.array_equal(slicethick, np.arange(len(slicethick)) * eachthick):
+        raise ValueError("slice tops must be 0, eachthick, 2 eachthick, ... (as ToTem's slicing dialog writes them)")
+    extent = tuple(float(v) for v in atoms[:, 1:4].max(axis=0)) if len(atoms) else (0.0, 0.0, 0.0)
+    st = specimen.Structure(atoms, extent, float(eachthick), len(slicethick))
+    spec = optics.ProbeSpec(kv=kv, semi_angle_mrad=semi_angle,
+                            aberrations=optics.Aberrations(focus=defocus_nm, Cs=c3_um * 1e3))
+    begin = ((p - (n + (raster[0] - 1) * step)) // 2, (p - (n + (raster[1] - 1) * step)) // 2)
+    req = _stem_request(st, flag, kv, sampling, n, p, step, raster, begin, detectors, spec, mid_layer=mid_layer,
+                        multiceng=multiceng, native_slicing=native_slicing)
+    return req
+
+
 def build_small_stem(n: int = 64, p: int = 128, raster=(3, 4), step: int = 5, slices: int = 6,
                      flag: str = PENG, kv: float = 200.0, sampling: float = 0.2,
                      detectors=((40.0, 150.0), (0.0, 15.0), (15.0, 40.0)), mid_layer=(2, 4),
