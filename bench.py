@@ -289,6 +289,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-comparators", action="store_true", help="skip the plain cuFFT and serving legs")
+    ap.add_argument("--no-band-skip", action="store_true",
+                    help="compute the wave columns the propagator zeroes too (totem_set_band_skip(0))")
     ns = ap.parse_args()
     if ns.impl == "reference":
         run_reference(ns)
@@ -308,6 +310,8 @@ def main():
     else:
         torch.cuda.set_device(local)
     from totem_b200 import capi
+    if ns.no_band_skip:
+        capi.set_band_skip(False)
     path = capi.PATH_FUSED if ns.path == "fused" else capi.PATH_PLAIN
     req = build_workload(ns.workload, raster=ns.raster)
     # a dedicated stream: the engine launches on it and the CUDA events below are recorded on it

@@ -202,6 +202,14 @@ TOTEM_API int totem_set_tx_builder(int mode, size_t scratch_bytes);
  * counterpart in the reference.  Runs on the legacy default stream, or on a stream the caller is
  * capturing, are never graphed. */
 TOTEM_API int totem_set_slice_graphs(int enable);
+/* The fused slice loop skips the wave's columns on which the propagator is zero in every row
+ * (beyond the 2/3-of-Nyquist cut of the reference's propagator, ToTEM_submit_v1.m:1558-1564, about
+ * a third of them; half with the HRTEM 1/2 cut): after the column pass multiplies by the
+ * propagator they are zero whatever the wave was, so they are neither read, transformed nor
+ * written, and the detector sums leave out their (zero) contributions.  The band is found from
+ * the propagator the caller passes; results equal those with every column computed.  1 = on
+ * (default), 0 = off.  Process-wide; no counterpart in the reference. */
+TOTEM_API int totem_set_band_skip(int enable);
 /* The gridding builder's batch plan, without a device (tests): jobs are numbered in slice order,
  * slice s owning jobs [job_beg[s], job_beg[s+1]); at most jobs_per_batch jobs run per batch.
  * Writes up to max_batches rows (s_lo, s_hi, j_lo, j_hi) to ``out`` and the batch count to

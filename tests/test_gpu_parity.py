@@ -179,3 +179,48 @@ def test_path_used_is_reported_and_fused_only_refuses_cufft(engine_lib):
     s.run(path=capi.PATH_PLAIN)
     assert s.timing().slice_path == capi.PATH_PLAIN
     s.close()
+
+
+@pytest.mark.parametrize("n,p,variant,focal", [(64, 128, 0, 1), (64, 128, 5, 3), (128, 256, 2, 1), (128, 256, 6, 1),
+                                                (256, 512, 0, 2)])
+def test_zero_band_skip_changes_nothing(engine_lib, n, p, variant, focal):
+    # The propagator is zero beyond 2/3 of Nyquist, so about a third of the wave's columns are
+    # zero after every column pass; skipping them (reads, transforms, writes, detector partials)
+    # must give the same numbers as computing them.
+    req = request.build_small_stem(n=n, p=p, raster=(2, 3), step=9, slices=5, sampling=0.1, mid_layer=(2, 5),
+                                   focal_steps=focal)
+    outs = {}
+    for skip in (False, True):
+        capi.set_band_skip(skip)
+        try:
+            s = capi.Session()
+            s.upload(req)
+            s.run(col_variant=variant)
+            outs[skip] = s.download()[:2]
+            s.close()
+        finally:
+            capi.set_band_skip(True)
+    for a, b in zip(outs[False], outs[True]):
+        np.testing.assert_array_equal(a, b)
+    _check(req, *outs[True])
+
+
+def test_zero_band_skip_hrtem_and_server(engine_lib):
+    # HRTEM's propagator is cut at 1/2 of Nyquist: half of the columns are skipped; the kept
+    # spectrum of the last pass is stored whole.  The server applies the same skip per group.
+    req, hs = request.build_si_hrtem_001(cells=(2, 2, 2), p=128, slices=6)
+    capi.set_band_skip(False)
+    try:
+        ex0, img0 = capi.hrtem_run(req, hs)
+        stem = request.build_small_stem(raster=(3, 3), mid_layer=(3,))
+        r0, m0 = capi.stem_run(stem)
+    finally:
+        capi.set_band_skip(True)
+    ex1, img1 = capi.hrtem_run(req, hs)
+    np.testing.assert_array_equal(ex0, ex1)
+    np.testing.assert_array_equal(img0, img1)
+    with capi.Server() as srv:
+        t = srv.submit(stem)
+        r1, m1 = srv.wait(t)
+    np.testing.assert_array_equal(r0, r1)
+    np.testing.assert_array_equal(m0, m1)

@@ -152,6 +152,7 @@ def load() -> C.CDLL:
                                     C.c_int, C.c_int, C.c_double, _dp, _dp]
     lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
     lib.totem_set_slice_graphs.argtypes = [C.c_int]
+    lib.totem_set_band_skip.argtypes = [C.c_int]
     llp = C.POINTER(C.c_longlong)
     lib.totem_slice_rows.argtypes = [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_double, _dp, C.c_int, C.c_int, C.c_int,
                                      _dp, C.c_longlong, _dp, C.c_longlong, _dp, _dp, llp, llp]
@@ -166,7 +167,7 @@ def load() -> C.CDLL:
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
-                 "totem_grid_batches", "totem_set_slice_graphs", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
+                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -539,6 +540,11 @@ def frozen_phonon(table, eachthick: float, slicethick, seed: int) -> np.ndarray:
 
 
 TX_AUTO, TX_DIRECT, TX_GRIDDING, TX_ROWS = 0, 1, 2, 3
+
+
+def set_band_skip(enable: bool):
+    """``totem_set_band_skip``: skip the wave columns the propagator zeroes (default on)."""
+    check(load().totem_set_band_skip(1 if enable else 0))
 
 
 def set_slice_graphs(enable: bool):

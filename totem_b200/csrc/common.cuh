@@ -147,6 +147,37 @@ std::vector<float2> stage_twiddles(int n);
 // ---------------------------------------------------------------------------------------------
 // Fused multislice
 // ---------------------------------------------------------------------------------------------
+// Spectral band of a propagator H [N][N] (FFT order): the columns c with band < c < N - band hold
+// zeros in every row, so after the column pass's multiply by H those columns of the wave are zero
+// whatever the wave was.  The reference's propagator is cut at 2/3 of Nyquist
+// (ToTEM_submit_v1.m:1558-1564), which makes about a third of the columns zero (half with the
+// HRTEM propagator's 1/2 limit).  The fused passes neither read, transform nor write them (the row
+// pass loads zeros there, the column pass skips the tiles that lie wholly inside that range), and
+// the detector sums skip those tiles, whose partial sums would be exact zeros: the results are
+// the same as with every column computed.  kNoBand: no column is known to be zero.
+constexpr int kNoBand = 1 << 30;
+__host__ __device__ __forceinline__ bool in_zero_band(int c, int band, int n) { return c > band && c < n - band; }
+// Column tiles of width n / nblk that lie wholly inside the zero band: [z0, z0 + nskip).
+struct TileSkip {
+  int z0 = 0, nskip = 0;
+};
+inline TileSkip zero_tiles(int n, int nblk, int band) {
+  TileSkip t;
+  if (nblk <= 0 || band >= n / 2) return t;
+  const int g = n / nblk;
+  const int first = (band + 1 + g - 1) / g;  // first tile starting after column ``band``
+  const int end = (n - band) / g;            // tiles [first, end) end at or before column n-band-1
+  if (end > first) {
+    t.z0 = first;
+    t.nskip = end - first;
+  }
+  return t;
+}
+// The band of H given as re/im planes [h][w] (host, FP64 inputs of the request).
+int spectral_band(const double* re, const double* im, int h, int w);
+// Process-wide: skip the zero band (totem_set_band_skip; on by default).
+bool band_skip_enabled();
+
 struct SliceLoopArgs {
   int n = 0;                       // window edge N (power of two)
   int items = 0;                   // items in this batch
@@ -164,6 +195,7 @@ struct SliceLoopArgs {
   double* part_exit = nullptr;
   int col_variant = 0;             // column-pass variant (multislice.cu, col_pass)
   int t_bf16 = 0;                  // the transmission slices are bfloat16 pairs, not complex64
+  int band = kNoBand;              // zero band of prop (spectral_band), kNoBand = none
 };
 // Number of column tiles per item (detector partial sums per probe) of a column-pass variant.
 int col_blocks(int n, int variant = 0);
@@ -192,11 +224,13 @@ struct GroupDesc {
   int slices;
   int aper_num;
   int exit_event;
+  int band;                     // zero band of prop (kNoBand = none)
 };
 Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                          const float2* tw, cudaStream_t st);
+// ``skip``: column tiles left out of the launch, wholly inside the zero band of every group in it
 Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
-                         const float2* tw, cudaStream_t st);
+                         const float2* tw, TileSkip skip, cudaStream_t st);
 
 // HRTEM imaging from the exit-wave spectrum spec [N][N] (FFT order): the exit wave
 // IFFT2(spec)/N^2 (complex64), and the image sum_k w_k |IFFT2(spec .* tf_k)/N^2|^2 (float32).
@@ -205,9 +239,10 @@ Status launch_exit_wave(int n, const float2* spec, float2* work, float2* out, co
 Status launch_tcc_image(int n, const float2* spec, const float2* tf, int planes, const double* w, float2* work,
                         float* out, const float2* tw, cudaStream_t st);
 
-// Sum the per-column-block partials in a fixed order: acc[(w*A + a)*depth + pos].
+// Sum the per-column-block partials in a fixed order: acc[(w*A + a)*depth + pos].  Tiles
+// [skip.z0, skip.z0 + skip.nskip) are left out (zero-band tiles: zero or never written).
 Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth,
-                         double* acc, cudaStream_t st);
+                         double* acc, cudaStream_t st, TileSkip skip = TileSkip());
 // out[i] = sum_w gfsf[w] * acc[w*AD + i], w in ascending order (accumulate_result).
 Status launch_combine(const double* acc, const double* gfsf, int w_num, long ad, double* out, cudaStream_t st);
 

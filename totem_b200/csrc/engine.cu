@@ -38,6 +38,7 @@ namespace {
 thread_local std::string g_last_error;
 std::atomic<int> g_tx_mode{TOTEM_TX_AUTO};
 std::atomic<int> g_slice_graphs{1};
+std::atomic<int> g_band_skip{1};
 std::atomic<size_t> g_tx_scratch{0};
 
 int fail(const Status& s) {
@@ -138,6 +139,7 @@ void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
 
 int totem::tx_builder_mode() { return g_tx_mode.load(); }
 bool totem::slice_graphs_enabled() { return g_slice_graphs.load() != 0; }
+bool totem::band_skip_enabled() { return g_band_skip.load() != 0; }
 size_t totem::tx_gridding_scratch() {
   const size_t b = g_tx_scratch.load();
   return b ? b : (1ull << 30);
@@ -308,6 +310,7 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
     for (size_t i = 0; i < vol; ++i) hp[i] = make_float2((float)a->prop_re[i], (float)a->prop_im[i]);
     TOTEM_TRY(upload(probe, pr, st));
     TOTEM_TRY(upload(prop, hp, st));
+    band = (h == w) ? totem::spectral_band(a->prop_re, a->prop_im, h, w) : totem::kNoBand;
     // exit detector: ifftshift(aper) (the reference shifts the wave instead, cuda_source_lobato.cu:1415)
     std::vector<float> me(vol * std::max(aper_num, 1)), mm;
     for (int q = 0; q < aper_num; ++q)
@@ -539,6 +542,9 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   }
   *batch_used = B;
   const int nblk = fused ? totem::col_blocks(h, col_variant) : 64;
+  // the zero band of the propagator: columns the fused passes skip, tiles the detector sums skip
+  const int band_run = (fused && totem::band_skip_enabled()) ? band : totem::kNoBand;
+  const totem::TileSkip skip = fused ? totem::zero_tiles(h, nblk, band_run) : totem::TileSkip();
   TOTEM_TRY(psi.ensure((size_t)B * vol * sizeof(float2)));
   TOTEM_TRY(part.ensure((size_t)n_events * B * aper_num * nblk * sizeof(double)));
   TOTEM_TRY(acc.ensure((size_t)n_events * w_num * ad * sizeof(double)));
@@ -569,6 +575,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
         s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
         s.col_variant = col_variant;
         s.t_bf16 = (t_storage == TOTEM_T_BF16);
+        s.band = band_run;
         TOTEM_TRY(prof_begin());
         TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
         TOTEM_TRY(prof_end(0));
@@ -623,7 +630,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
       }
       for (int e = 0; e < n_events; ++e) {
         TOTEM_TRY(totem::launch_det_reduce(part_e + e * part_stride, nblk, aper_num, items, (int)item0, depth,
-                                           acc.as<double>() + (size_t)e * w_num * ad, stream));
+                                           acc.as<double>() + (size_t)e * w_num * ad, stream, skip));
         ++*launches;
       }
     }
@@ -636,7 +643,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
     // what the launches embed: sizes, buffer addresses and the detection events
     std::vector<long long> key = {h, items_total, B, slices, col_variant, t_storage, n_events, exit_event, aper_num,
                                   w_num, depth, nblk, L, p_h, p_w, begin_row, begin_col, step, width_red,
-                                  (long long)tslice_bytes};
+                                  (long long)tslice_bytes, band_run};
     for (const void* q : {(const void*)psi.p, (const void*)part.p, (const void*)acc.p, (const void*)probe.p,
                           (const void*)prop.p, (const void*)tw_n.p, (const void*)mask_mid.p, (const void*)mask_exit.p,
                           Tslices, (const void*)gfsf_d.p, (const void*)out_result.p, (const void*)out_mid.p})
@@ -775,6 +782,7 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
   s.tw = tw_pw.as<float2>();
   s.aper_num = 0;
   s.t_bf16 = (hr->t_storage == TOTEM_T_BF16);
+  s.band = totem::band_skip_enabled() ? totem::spectral_band(hr->prop_re, hr->prop_im, n, n) : totem::kNoBand;
   auto tslice = [&](int k) { return static_cast<const char*>(Tslices) + (size_t)k * tslice_bytes; };
   // psi = wave .* T_0, then per slice FFT2 .* psf_fft IFFT2 .* T_{k+1}; the last column pass keeps
   // the spectrum FFT2(psi_{S-1} .* T) .* psf_fft, whose IFFT2 is the exit wave
@@ -1109,6 +1117,13 @@ int totem_set_tx_builder(int mode, size_t scratch_bytes) {
 int totem_set_slice_graphs(int enable) {
   if (enable != 0 && enable != 1) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "enable must be 0 or 1"));
   g_slice_graphs.store(enable);
+  g_last_error.clear();
+  return TOTEM_OK;
+}
+
+int totem_set_band_skip(int enable) {
+  if (enable != 0 && enable != 1) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "enable must be 0 or 1"));
+  g_band_skip.store(enable);
   g_last_error.clear();
   return TOTEM_OK;
 }

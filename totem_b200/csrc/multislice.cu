@@ -29,11 +29,13 @@ namespace {
 // One CTA's share of a row pass: rows row0 .. row0+G-1 of one probe's wave.
 //   psi_item  the probe's wave [N][N];  t_origin  T at the window origin (row stride p_w),
 //   complex64 or, with TB16, bfloat16 pairs;  probe_item  the probe [N][N] (FIRST only: the first
-//   pass starts from the probe).
+//   pass starts from the probe);  band  the zero band of the propagator: the wave's columns
+//   band < c < N - band are zero after the column pass, so they are neither loaded (zeros
+//   instead) nor stored (the column pass does not read them).
 template <int N, bool FIRST, bool TB16 = false>
 __device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const void* __restrict__ t_origin, long p_w,
                                          const float2* __restrict__ probe_item, int row0, float scale,
-                                         const float2* __restrict__ tw) {
+                                         const float2* __restrict__ tw, int band) {
   using TElem = std::conditional_t<TB16, __nv_bfloat162, float2>;
   constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T;
   extern __shared__ float2 sh[];
@@ -66,7 +68,7 @@ __device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const vo
     for (int m = 0; m < P; ++m) v[m] = __ldg(src + j + m * T);
   } else {
 #pragma unroll
-    for (int m = 0; m < P; ++m) v[m] = prow[j + m * T];
+    for (int m = 0; m < P; ++m) v[m] = in_zero_band(j + m * T, band, N) ? make_float2(0.f, 0.f) : prow[j + m * T];
   }
   __syncthreads();  // twiddles staged
   if (!FIRST) fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync, prefetch_t);
@@ -81,7 +83,8 @@ __device__ __forceinline__ void row_tile(float2* __restrict__ psi_item, const vo
   sync();  // every thread of the transform has read its window values before the region is reused
   fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
-  for (int m = 0; m < P; ++m) prow[j + m * T] = v[m];
+  for (int m = 0; m < P; ++m)
+    if (!in_zero_band(j + m * T, band, N)) prow[j + m * T] = v[m];
 }
 
 template <int N, bool FIRST, bool TB16>
@@ -97,7 +100,7 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
   const int y0 = a.geo.begin_col + (pos % a.geo.width_red) * a.geo.step;
   row_tile<N, FIRST, TB16>(a.psi + (long)item * N * N,
                            static_cast<const TElem*>(tslice) + (long)x0 * a.geo.p_width + y0, a.geo.p_width,
-                           a.probe + (long)w * N * N, row0, scale, a.tw);
+                           a.probe + (long)w * N * N, row0, scale, a.tw, a.band);
 }
 
 // Deterministic block sum of one double per thread; result valid in thread 0.
@@ -143,10 +146,12 @@ struct ColInputs {
 
 // One CTA's share of a column pass: columns cb*G .. cb*G+G-1 of one probe's wave.  ``item`` is
 // the item's index in the partial-sum arrays.  flags: 1 mid detectors, 2 exit detectors,
-// 4 final pass (no inverse transform), 8 (with 4) store the spectrum.
+// 4 final pass (no inverse transform), 8 (with 4) store the spectrum.  A column inside the zero
+// band (band < c < N - band; the propagator is zero on it) is taken as zero, not loaded, and not
+// stored, except that a kept spectrum (flag 8) is stored whole.
 template <int N, bool PREFETCH, int G>
 __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const ColInputs& in, int item, int cb, int flags,
-                                         const float2* __restrict__ tw) {
+                                         const float2* __restrict__ tw, int band) {
   constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T;
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
@@ -155,11 +160,12 @@ __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const Co
   constexpr int nblk = N / G;
   const int j = threadIdx.x / G, g = threadIdx.x - j * G;
   const int c = cb * G + g;
+  const bool zc = in_zero_band(c, band, N);
   load_twiddles<N>(s_tw, tw);
   float2* base = psi_item + c;
   float2 v[P];
 #pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = base[(long)(j + m * T) * N];
+  for (int m = 0; m < P; ++m) v[m] = zc ? make_float2(0.f, 0.f) : base[(long)(j + m * T) * N];
   __syncthreads();
   const ColLayout<N, G> L;
   const SyncBlock sync;
@@ -196,8 +202,10 @@ __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const Co
     return;
   }
   fft_regs<N, true>(v, j, g, s_tw, s_x, L, sync);
+  if (!zc) {
 #pragma unroll
-  for (int m = 0; m < P; ++m) base[(long)(j + m * T) * N] = v[m];
+    for (int m = 0; m < P; ++m) base[(long)(j + m * T) * N] = v[m];
+  }
 }
 
 // Column-pass variants, per 2048-probe launch on the SrTiO3 512^2 workload (microseconds per
@@ -209,14 +217,17 @@ __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const Co
 // 1.24: the pass needs warps more than it needs its loads hidden.  With 8-column tiles,
 // prefetching the propagator into shared memory (4.6 ms against 4.3 ms per 4096 probes) and an
 // 80-register cap (5.8 ms) were slower.
+// The launch covers the tiles outside [skip.z0, skip.z0 + skip.nskip) only.
 template <int N, bool PREFETCH, int CTAS128, int GW>
 __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
-    k_col_pass(SliceLoopArgs a, int flags) {
+    k_col_pass(SliceLoopArgs a, int flags, TileSkip skip) {
   constexpr int G = ColCfg<N, CTAS128, GW>::G;
   constexpr int nblk = N / G;
-  const int item = blockIdx.x / nblk, cb = blockIdx.x - item * nblk;
+  const int active = nblk - skip.nskip;
+  const int item = blockIdx.x / active, t = blockIdx.x - item * active;
+  const int cb = t < skip.z0 ? t : t + skip.nskip;
   const ColInputs in{a.prop, a.mask_mid, a.mask_exit, a.aper_num, a.part_mid, a.part_exit};
-  col_tile<N, PREFETCH, G>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw);
+  col_tile<N, PREFETCH, G>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw, a.band);
 }
 
 // Group of launch item ``li``: the last g with item_begin[g] <= li.
@@ -251,9 +262,9 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
   const float2* t_origin = d.t_stack + (long)slice * d.p_h * p_w + (long)x0 * p_w + y0;
   float2* psi_item = d.psi + (long)item * N * N;
   if (slice == 0)
-    row_tile<N, true>(psi_item, t_origin, p_w, d.probe + (long)w * N * N, row0, 1.f, tw);
+    row_tile<N, true>(psi_item, t_origin, p_w, d.probe + (long)w * N * N, row0, 1.f, tw, d.band);
   else
-    row_tile<N, false>(psi_item, t_origin, p_w, nullptr, row0, 1.f / ((float)N * (float)N), tw);
+    row_tile<N, false>(psi_item, t_origin, p_w, nullptr, row0, 1.f / ((float)N * (float)N), tw, d.band);
 }
 
 // Column pass of a continuous batch: detectors at the group's mid-layer slices, exit detectors
@@ -261,9 +272,11 @@ __global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
 template <int N>
 __global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB)
     k_col_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
-                 const float2* __restrict__ tw) {
+                 const float2* __restrict__ tw, TileSkip skip) {
   constexpr int G = ColCfg<N>::G, nblk = N / G;
-  const int li = blockIdx.x / nblk, cb = blockIdx.x - li * nblk;
+  const int active = nblk - skip.nskip;
+  const int li = blockIdx.x / active, t = blockIdx.x - li * active;
+  const int cb = t < skip.z0 ? t : t + skip.nskip;
   const int gidx = find_group(item_begin, ngroups, li);
   const GroupDesc& d = groups[gidx];
   const int item = li - __ldg(item_begin + gidx);
@@ -280,17 +293,18 @@ __global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB)
     flags |= 2 | 4;
     in.part_exit = d.part + d.exit_event * estride;
   }
-  col_tile<N, false, G>(d.psi + (long)item * N * N, in, item, cb, flags, tw);
+  col_tile<N, false, G>(d.psi + (long)item * N * N, in, item, cb, flags, tw, d.band);
 }
 
 __global__ void k_det_reduce(const double* __restrict__ part, int nblk, int aper_num, int items, int item0,
-                             int depth, double* __restrict__ acc) {
+                             int depth, double* __restrict__ acc, TileSkip skip) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= items * aper_num) return;
   const int item = t / aper_num, a = t - item * aper_num;
   const double* p = part + (long)t * nblk;
   double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += p[b];
+  for (int b = 0; b < nblk; ++b)
+    if (b < skip.z0 || b >= skip.z0 + skip.nskip) s += p[b];
   const int gi = item0 + item;
   const int w = gi / depth, pos = gi - w * depth;
   acc[((long)w * aper_num + a) * depth + pos] = s;
@@ -326,7 +340,10 @@ Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   constexpr int G = ColCfg<N, CTAS128, GW>::G, T = ColCfg<N>::T;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128, GW>, smem));
-  k_col_pass<N, PREFETCH, CTAS128, GW><<<(unsigned)((long)a.items * (N / G)), G * T, smem, st>>>(a, flags);
+  // a kept spectrum is stored whole: no tile is left out then
+  const TileSkip skip = (flags & 8) ? TileSkip() : zero_tiles(N, N / G, a.band);
+  k_col_pass<N, PREFETCH, CTAS128, GW>
+      <<<(unsigned)((long)a.items * (N / G - skip.nskip)), G * T, smem, st>>>(a, flags, skip);
   return cuda_status(cudaGetLastError(), "k_col_pass");
 }
 
@@ -436,11 +453,14 @@ Status row_groups(const GroupDesc* groups, const int* item_begin, int ngroups, l
 
 template <int N>
 Status col_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
-                  cudaStream_t st) {
+                  TileSkip skip, cudaStream_t st) {
   constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_col_groups<N>, smem));
-  k_col_groups<N><<<(unsigned)(items * (N / G)), G * T, smem, st>>>(groups, item_begin, ngroups, tick, tw);
+  if (skip.nskip < 0 || skip.z0 < 0 || skip.z0 + skip.nskip > N / G)
+    return Status::Err(TOTEM_ERR_STATE, "column tiles to skip out of range");
+  k_col_groups<N><<<(unsigned)(items * (N / G - skip.nskip)), G * T, smem, st>>>(groups, item_begin, ngroups, tick,
+                                                                                 tw, skip);
   return cuda_status(cudaGetLastError(), "k_col_groups");
 }
 
@@ -459,25 +479,39 @@ Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, 
 }
 
 Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
-                         const float2* tw, cudaStream_t st) {
+                         const float2* tw, TileSkip skip, cudaStream_t st) {
   if (items <= 0 || ngroups <= 0) return Status::Ok();
   switch (n) {
-    case 64: return col_groups<64>(groups, item_begin, ngroups, items, tick, tw, st);
-    case 128: return col_groups<128>(groups, item_begin, ngroups, items, tick, tw, st);
-    case 256: return col_groups<256>(groups, item_begin, ngroups, items, tick, tw, st);
-    case 512: return col_groups<512>(groups, item_begin, ngroups, items, tick, tw, st);
-    case 1024: return col_groups<1024>(groups, item_begin, ngroups, items, tick, tw, st);
-    case 2048: return col_groups<2048>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 64: return col_groups<64>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 128: return col_groups<128>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 256: return col_groups<256>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 512: return col_groups<512>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 1024: return col_groups<1024>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 2048: return col_groups<2048>(groups, item_begin, ngroups, items, tick, tw, skip, st);
   }
   return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
 }
 
 Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth, double* acc,
-                         cudaStream_t st) {
+                         cudaStream_t st, TileSkip skip) {
   const int n = items * aper_num;
   if (n == 0) return Status::Ok();
-  k_det_reduce<<<(n + 127) / 128, 128, 0, st>>>(part, nblk, aper_num, items, item0, depth, acc);
+  k_det_reduce<<<(n + 127) / 128, 128, 0, st>>>(part, nblk, aper_num, items, item0, depth, acc, skip);
   return cuda_status(cudaGetLastError(), "k_det_reduce");
+}
+
+int spectral_band(const double* re, const double* im, int h, int w) {
+  int band = 0;
+  for (int c = 0; c < w; ++c) {
+    const int dist = c < w - c ? c : w - c;
+    if (dist <= band) continue;
+    for (int r = 0; r < h; ++r)
+      if (re[(size_t)r * w + c] != 0.0 || im[(size_t)r * w + c] != 0.0) {
+        band = dist;
+        break;
+      }
+  }
+  return band;
 }
 
 Status launch_combine(const double* acc, const double* gfsf, int w_num, long ad, double* out, cudaStream_t st) {

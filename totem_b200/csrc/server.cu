@@ -57,6 +57,7 @@ struct Request {
   totem::DetectionEvents de;
   long long items = 0, items_left = 0;
   int nblk = 0;
+  int band = totem::kNoBand;        // zero band of the request's propagator used by its launches
   size_t item_bytes = 0;
   long long probe_slices = 0;
   double est = 0;                   // estimated device seconds (preparation order)
@@ -246,6 +247,7 @@ Status totem_server::prepare(Request* r) {
   r->items = (s->aper_num > 0) ? (long long)s->w_num * s->depth : 0;
   r->items_left = r->items;
   r->nblk = totem::col_blocks(s->h);
+  r->band = totem::band_skip_enabled() ? s->band : totem::kNoBand;
   r->item_bytes = (size_t)s->h * s->w * sizeof(float2) + (size_t)r->de.n_events * s->aper_num * r->nblk * sizeof(double);
   r->probe_slices = (long long)s->w_num * s->depth * s->slices;
   TOTEM_CUDA(cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming));
@@ -377,6 +379,9 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
     auto* desc = reinterpret_cast<totem::GroupDesc*>(h + desc_off);
     auto* ib = reinterpret_cast<int*>(h + ib_off);
     long long items = 0;
+    // column tiles left out of the column launch: those in the zero band of every group
+    const int nblk_n = totem::col_blocks(n);
+    int skip_lo = 0, skip_hi = nblk_n;
     for (size_t i = 0; i < ng; ++i) {
       const totem::PlanGroup& g = *gs[i];
       Request* r = nullptr;
@@ -399,6 +404,10 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
       x.slices = s->slices;
       x.aper_num = s->aper_num;
       x.exit_event = r->de.exit_event;
+      x.band = r->band;
+      const totem::TileSkip zt = totem::zero_tiles(n, nblk_n, r->band);
+      skip_lo = std::max(skip_lo, zt.z0);
+      skip_hi = std::min(skip_hi, zt.z0 + zt.nskip);
       ib[i] = (int)items;
       items += g.items;
     }
@@ -407,7 +416,12 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
     const auto* dd = reinterpret_cast<const totem::GroupDesc*>(d + desc_off);
     const auto* dib = reinterpret_cast<const int*>(d + ib_off);
     TOTEM_TRY(totem::launch_row_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
-    TOTEM_TRY(totem::launch_col_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
+    totem::TileSkip skip;
+    if (skip_hi > skip_lo) {
+      skip.z0 = skip_lo;
+      skip.nskip = skip_hi - skip_lo;
+    }
+    TOTEM_TRY(totem::launch_col_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), skip, sst));
     launched += 2;
   }
   // groups that ran their last slice: detector sums, then their wave memory goes back
@@ -420,7 +434,8 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
     for (int e = 0; e < r->de.n_events; ++e)
       TOTEM_TRY(totem::launch_det_reduce(static_cast<const double*>(g.part) + e * estride, r->nblk, s->aper_num,
                                          g.items, (int)g.item0, s->depth,
-                                         s->acc.as<double>() + (size_t)e * s->w_num * ad, sst));
+                                         s->acc.as<double>() + (size_t)e * s->w_num * ad, sst,
+                                         totem::zero_tiles(s->h, r->nblk, r->band)));
     launched += r->de.n_events;
     TOTEM_CUDA(cudaFreeAsync(g.psi, sst));
     TOTEM_CUDA(cudaFreeAsync(g.part, sst));

@@ -193,6 +193,8 @@ struct totem_session {
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   TotemTiming timing{};
   long long h2d_bytes = 0, d2h_bytes = 0;
+  // zero band of the uploaded propagator (totem::spectral_band), kNoBand if none is known
+  int band = totem::kNoBand;
   // which implementations the last run used (TotemTiming.slice_path / tx_fft_path / tx_builder)
   int ran_slice_path = -1, ran_tx_fft = -1, ran_tx_builder = -1;
   // per-launch profiling of the fused passes (TotemRunOptions.profile)
