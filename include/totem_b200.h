@@ -121,14 +121,20 @@ enum {
 /* Engine options of one run (defaults: all zero). */
 typedef struct TotemRunOptions {
   int path;                        /* TOTEM_PATH_*                                              */
-  int batch;                       /* probes in flight per batch, 0 = engine's choice          */
+  int batch;                       /* probes in flight per batch, 0 = the tuned choice (else up to
+                                      4 GiB of waves for the fused path, 1 GiB for cuFFT)         */
   int skip_transmission;           /* 1 = reuse the transmission built by an earlier run        */
   int profile;                     /* 1 = CUDA events around every slice-loop pass launch       */
-  int col_variant;                 /* fused column pass: 0 = engine default (propagator read from
-                                      L2, 16-column tiles up to N = 512), 2 = propagator prefetched
-                                      to shared memory, 3 = 80-register cap (more resident CTAs),
-                                      5 = 8-column tiles, 6 = 32-column tiles (N <= 512)           */
+  int col_variant;                 /* fused column pass: 0 = the tuned choice for this window and
+                                      GPU (totem_load_tuning), else 1; 1 = built-in default
+                                      (propagator read from L2, 16-column tiles up to N = 512,
+                                      8 above), 2 = propagator prefetched to shared memory,
+                                      3 = 80-register cap (more resident CTAs), 5 = 8-column tiles,
+                                      6 = 32-column tiles (N <= 512)                             */
   int t_storage;                   /* TOTEM_T_* (fused path only)                                */
+  int row_variant;                 /* fused row pass: 0 = the tuned choice, else 1; 1 = built-in
+                                      default; 3, 4, 5 = registers sized for that many resident
+                                      128-thread CTAs per SM (3: N >= 1024, 5: N <= 1024)         */
 } TotemRunOptions;
 
 /* Device times (CUDA events) of the last run, milliseconds. */
@@ -147,6 +153,7 @@ typedef struct TotemTiming {
   int slice_path;                  /* TOTEM_PATH_FUSED or TOTEM_PATH_PLAIN (cuFFT)               */
   int tx_fft_path;                 /* transmission inverse FFT: TOTEM_PATH_FUSED or _PLAIN (cuFFT) */
   int tx_builder;                  /* TOTEM_TX_DIRECT, TOTEM_TX_GRIDDING or TOTEM_TX_ROWS          */
+  int row_variant, col_variant;    /* fused pass variants used (after the tuning table)          */
 } TotemTiming;
 
 typedef struct totem_session totem_session;
@@ -210,6 +217,18 @@ TOTEM_API int totem_set_slice_graphs(int enable);
  * the propagator the caller passes; results equal those with every column computed.  1 = on
  * (default), 0 = off.  Process-wide; no counterpart in the reference. */
 TOTEM_API int totem_set_band_skip(int enable);
+/* Launch shapes chosen by measurement (python -m totem_b200.tune writes the table): one JSON
+ * object per line, {"device": "<cudaDeviceProp.name>", "n": <window edge>, "row_variant": r,
+ * "col_variant": c, "batch_mib": b, ...}.  Runs whose TotemRunOptions leave row_variant,
+ * col_variant or batch at 0 use the entry of their GPU and window, and the built-in defaults where
+ * there is none.  The library loads totem_b200/data/tuning.jsonl beside its lib/ directory on first
+ * use (or the file named by TOTEM_TUNING_FILE); this call replaces the table with ``path`` (NULL
+ * or "" = no table: built-in defaults).  ``entries`` receives the number of entries read.
+ * Process-wide; no counterpart in the reference, which sizes its batch from free memory
+ * (cuda_source_lobato.cu:1250-1260). */
+TOTEM_API int totem_load_tuning(const char *path, int *entries);
+/* The launch shapes a fused run on ``device`` with an n x n window would use by default. */
+TOTEM_API int totem_tuned_config(int device, int n, int *row_variant, int *col_variant, long long *batch_bytes);
 /* The gridding builder's batch plan, without a device (tests): jobs are numbered in slice order,
  * slice s owning jobs [job_beg[s], job_beg[s+1]); at most jobs_per_batch jobs run per batch.
  * Writes up to max_batches rows (s_lo, s_hi, j_lo, j_hi) to ``out`` and the batch count to
@@ -385,6 +404,11 @@ typedef struct TotemServerOptions {
   int policy;                    /* TOTEM_SCHED_*                                              */
   int prep_threads;              /* host threads preparing requests (upload, transmission);
                                     0 = 2                                                      */
+  int mixed_windows;             /* 1 = at a tick with groups of more than one of the window
+                                    sizes 256^2, 512^2, 1024^2, all of them go through one
+                                    persistent row-pass and one column-pass launch whose CTAs
+                                    take tiles of any of these sizes from a queue; 0 = one launch
+                                    pair per window size.  Results are the same either way      */
 } TotemServerOptions;
 
 enum {

@@ -26,7 +26,9 @@ def mex_library(param: str, transmission: bool, out_dir: str = REF_OUT) -> C.CDL
         return None
     from totem_b200 import capi
     capi.load()  # the engine library first: the MEX builds link against it
-    lib = C.CDLL(path, mode=C.RTLD_GLOBAL)
+    # local symbol scope, as MATLAB loads MEX files: the four shim libraries export the same
+    # myProjectfun, and each MEX build must bind to the one it was linked against
+    lib = C.CDLL(path, mode=C.RTLD_LOCAL)
     vp = C.c_void_p
     lib.mexFunction.argtypes = [C.c_int, C.POINTER(vp), C.c_int, C.POINTER(vp)]
     lib.mexFunction.restype = None

@@ -58,7 +58,8 @@ def _c_layout(tmp_path, struct, fields):
     return dict((ln.split()[0], int(ln.split()[1])) for ln in out if ln.strip())
 
 
-@pytest.mark.parametrize("cls", [capi.TotemStemArgs, capi.TotemStemOut, capi.TotemRunOptions, capi.TotemTiming])
+@pytest.mark.parametrize("cls", [capi.TotemStemArgs, capi.TotemStemOut, capi.TotemRunOptions, capi.TotemTiming,
+                                 capi.TotemServerOptions])
 def test_struct_layout_matches_header(tmp_path, cls):
     names = [f[0] for f in cls._fields_]
     c = _c_layout(tmp_path, cls.__name__, names)

@@ -90,3 +90,29 @@ def test_many_requests_in_flight(engine_lib):
     for r, (res, mid) in zip(reqs, got):
         r0, m0 = capi.stem_run(r)
         assert np.array_equal(res, r0) and np.array_equal(mid, m0)
+
+
+def test_mixed_window_sizes_in_one_launch_equal_alone(engine_lib):
+    # 256^2, 512^2 and 1024^2 windows running at the same ticks go through one persistent
+    # row-pass and one column-pass launch (mixed_windows); each result must still equal the
+    # request alone bit for bit, with mid layers, defocus series and both parameterisations
+    reqs = [
+        request.build_small_stem(n=256, p=512, raster=(2, 2), step=30, slices=6, sampling=0.1, mid_layer=(2, 5)),
+        request.build_small_stem(n=512, p=1024, raster=(1, 3), step=64, slices=5, sampling=0.05, cells=4,
+                                 mid_layer=(3,), flag="l"),
+        request.build_small_stem(n=1024, p=1024, raster=(1, 1), step=0, slices=4, sampling=0.05, cells=4,
+                                 mid_layer=()),
+        request.build_small_stem(n=256, p=512, raster=(1, 2), step=40, slices=3, sampling=0.1, focal_steps=3,
+                                 mid_layer=(1,)),
+        request.build_small_stem(raster=(2, 2), slices=4, mid_layer=(2,)),  # 64^2: its own launches
+    ]
+    alone = [capi.stem_run(r) for r in reqs]
+    with capi.Server(device=0, mixed_windows=True) as srv:
+        tickets = [srv.submit(r) for r in reqs]
+        got = [srv.wait(t) for t in tickets]
+        stats = srv.stats()
+    for i, ((r0, m0), (r1, m1)) in enumerate(zip(alone, got)):
+        assert np.array_equal(r0, r1), i
+        assert np.array_equal(m0, m1), i
+    assert stats["requests_done"] == len(reqs)
+    _oracle_check(reqs[0], *got[0])

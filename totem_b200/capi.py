@@ -54,7 +54,7 @@ T_COMPLEX64, T_BF16 = 0, 1
 
 class TotemRunOptions(C.Structure):
     _fields_ = [("path", C.c_int), ("batch", C.c_int), ("skip_transmission", C.c_int), ("profile", C.c_int),
-                ("col_variant", C.c_int), ("t_storage", C.c_int)]
+                ("col_variant", C.c_int), ("t_storage", C.c_int), ("row_variant", C.c_int)]
 
 
 class TotemHrtemArgs(C.Structure):
@@ -72,13 +72,14 @@ class TotemTiming(C.Structure):
                 ("row_pass_ms", C.c_float), ("col_pass_ms", C.c_float),
                 ("row_pass_launches", C.c_int), ("col_pass_launches", C.c_int),
                 ("probe_slices", C.c_longlong), ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong),
-                ("slice_path", C.c_int), ("tx_fft_path", C.c_int), ("tx_builder", C.c_int)]
+                ("slice_path", C.c_int), ("tx_fft_path", C.c_int), ("tx_builder", C.c_int),
+                ("row_variant", C.c_int), ("col_variant", C.c_int)]
 
 
 class TotemServerOptions(C.Structure):
     _fields_ = [("struct_size", C.c_int), ("device", C.c_int), ("hbm_budget", C.c_ulonglong),
                 ("wave_bytes", C.c_ulonglong), ("chunk_bytes", C.c_ulonglong), ("ticks_ahead", C.c_int),
-                ("policy", C.c_int), ("prep_threads", C.c_int)]
+                ("policy", C.c_int), ("prep_threads", C.c_int), ("mixed_windows", C.c_int)]
 
 
 class TotemRequestInfo(C.Structure):
@@ -153,6 +154,9 @@ def load() -> C.CDLL:
     lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
     lib.totem_set_slice_graphs.argtypes = [C.c_int]
     lib.totem_set_band_skip.argtypes = [C.c_int]
+    lib.totem_load_tuning.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
+    lib.totem_tuned_config.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_longlong)]
     llp = C.POINTER(C.c_longlong)
     lib.totem_slice_rows.argtypes = [C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_double, _dp, C.c_int, C.c_int, C.c_int,
                                      _dp, C.c_longlong, _dp, C.c_longlong, _dp, _dp, llp, llp]
@@ -167,7 +171,7 @@ def load() -> C.CDLL:
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
-                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
+                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_load_tuning", "totem_tuned_config", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -283,8 +287,8 @@ class Session:
         check(self.lib.totem_session_upload(self.h, C.byref(self._m.args)))
 
     def run(self, what: int = 0, path: int = PATH_FUSED, batch: int = 0, skip_transmission: bool = False,
-            profile: bool = False, col_variant: int = 0, t_storage: int = T_COMPLEX64):
-        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile), col_variant, t_storage)
+            profile: bool = False, col_variant: int = 0, t_storage: int = T_COMPLEX64, row_variant: int = 0):
+        o = TotemRunOptions(path, batch, int(skip_transmission), int(profile), col_variant, t_storage, row_variant)
         check(self.lib.totem_session_run(self.h, what, C.byref(o)))
 
     def hrtem(self, spec, t_storage: int = T_COMPLEX64, exit_wave: bool = True, image: bool = True):
@@ -343,10 +347,11 @@ class Server:
     """
 
     def __init__(self, device: int = -1, hbm_budget: int = 0, wave_bytes: int = 0, chunk_bytes: int = 0,
-                 ticks_ahead: int = 0, policy: int = SCHED_SHORTEST, prep_threads: int = 0):
+                 ticks_ahead: int = 0, policy: int = SCHED_SHORTEST, prep_threads: int = 0,
+                 mixed_windows: bool = False):
         self.lib = load()
         o = TotemServerOptions(C.sizeof(TotemServerOptions), device, hbm_budget, wave_bytes, chunk_bytes,
-                               ticks_ahead, policy, prep_threads)
+                               ticks_ahead, policy, prep_threads, int(mixed_windows))
         h = C.c_void_p()
         check(self.lib.totem_server_create(C.byref(o), C.byref(h)))
         self.h = h
@@ -481,7 +486,7 @@ def stem_run(req, path: int = PATH_FUSED, batch: int = 0):
     res = np.zeros(req.aper_num * req.depth)
     mid = np.zeros(req.aper_num * req.depth * len(req.mid_layer))
     out = TotemStemOut(_ptr(res), _ptr(mid), None, None)
-    opt = TotemRunOptions(path, batch, 0, 0, 0, T_COMPLEX64)
+    opt = TotemRunOptions(path, batch, 0, 0, 0, T_COMPLEX64, 0)
     check(lib.totem_stem_run(C.byref(m.args), C.byref(opt), C.byref(out)))
     return res, mid
 
@@ -540,6 +545,25 @@ def frozen_phonon(table, eachthick: float, slicethick, seed: int) -> np.ndarray:
 
 
 TX_AUTO, TX_DIRECT, TX_GRIDDING, TX_ROWS = 0, 1, 2, 3
+
+
+def load_tuning(path: str | None) -> int:
+    """``totem_load_tuning``: replace the process's tuning table (None = no table); returns the
+    number of entries."""
+    n = C.c_int(0)
+    check(load().totem_load_tuning(path.encode() if path else None, C.byref(n)))
+    return n.value
+
+
+def tuned_config(n: int, device: int = 0):
+    """``totem_tuned_config``: (row_variant, col_variant, batch_bytes) a fused run with an n x n
+    window would use on ``device`` by default."""
+    r, c, b = C.c_int(0), C.c_int(0), C.c_longlong(0)
+    check(load().totem_tuned_config(device, n, C.byref(r), C.byref(c), C.byref(b)))
+    return r.value, c.value, b.value
+
+
+TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "tuning.jsonl")
 
 
 def set_band_skip(enable: bool):

@@ -147,35 +147,25 @@ std::vector<float2> stage_twiddles(int n);
 // ---------------------------------------------------------------------------------------------
 // Fused multislice
 // ---------------------------------------------------------------------------------------------
-// Spectral band of a propagator H [N][N] (FFT order): the columns c with band < c < N - band hold
-// zeros in every row, so after the column pass's multiply by H those columns of the wave are zero
+// Spectral band of a propagator H [N][N] (FFT order): the largest index distance from DC,
+// min(c, N - c), of a column holding a non-zero entry.  The columns c with band < c < N - band are
+// zero in every row, so after the column pass's multiply by H those columns of the wave are zero
 // whatever the wave was.  The reference's propagator is cut at 2/3 of Nyquist
-// (ToTEM_submit_v1.m:1558-1564), which makes about a third of the columns zero (half with the
-// HRTEM propagator's 1/2 limit).  The fused passes neither read, transform nor write them (the row
-// pass loads zeros there, the column pass skips the tiles that lie wholly inside that range), and
-// the detector sums skip those tiles, whose partial sums would be exact zeros: the results are
-// the same as with every column computed.  kNoBand: no column is known to be zero.
-constexpr int kNoBand = 1 << 30;
-__host__ __device__ __forceinline__ bool in_zero_band(int c, int band, int n) { return c > band && c < n - band; }
-// Column tiles of width n / nblk that lie wholly inside the zero band: [z0, z0 + nskip).
+// (ToTEM_submit_v1.m:1558-1564): band = N / 3.
+int spectral_band(const double* re, const double* im, int h, int w);
+// Column tiles [z0, z0 + nskip) left out of a column-pass launch.
 struct TileSkip {
   int z0 = 0, nskip = 0;
 };
-inline TileSkip zero_tiles(int n, int nblk, int band) {
-  TileSkip t;
-  if (nblk <= 0 || band >= n / 2) return t;
-  const int g = n / nblk;
-  const int first = (band + 1 + g - 1) / g;  // first tile starting after column ``band``
-  const int end = (n - band) / g;            // tiles [first, end) end at or before column n-band-1
-  if (end > first) {
-    t.z0 = first;
-    t.nskip = end - first;
-  }
-  return t;
-}
-// The band of H given as re/im planes [h][w] (host, FP64 inputs of the request).
-int spectral_band(const double* re, const double* im, int h, int w);
-// Process-wide: skip the zero band (totem_set_band_skip; on by default).
+// The fixed zero-band columns of an n x n window (BandCols in fft.cuh; lo = hi: none).
+void band_columns(int n, int* lo, int* hi);
+// Whether a request with propagator band ``band`` may skip band_columns(n) with the column-pass
+// variant ``col_variant``: the columns lie in its zero band and the variant's tiles cover them
+// whole.
+bool band_skip_ok(int n, int band, int col_variant);
+// The tiles of width n / nblk inside band_columns(n).
+TileSkip band_tiles(int n, int nblk);
+// Process-wide: skip the zero band where band_skip_ok (totem_set_band_skip; on by default).
 bool band_skip_enabled();
 
 struct SliceLoopArgs {
@@ -195,7 +185,8 @@ struct SliceLoopArgs {
   double* part_exit = nullptr;
   int col_variant = 0;             // column-pass variant (multislice.cu, col_pass)
   int t_bf16 = 0;                  // the transmission slices are bfloat16 pairs, not complex64
-  int band = kNoBand;              // zero band of prop (spectral_band), kNoBand = none
+  int skip_band = 0;               // 1: the passes leave out band_columns(n) (band_skip_ok)
+  int row_variant = 0;             // row-pass variant (multislice.cu, row_pass)
 };
 // Number of column tiles per item (detector partial sums per probe) of a column-pass variant.
 int col_blocks(int n, int variant = 0);
@@ -224,10 +215,25 @@ struct GroupDesc {
   int slices;
   int aper_num;
   int exit_event;
-  int band;                     // zero band of prop (kNoBand = none)
+  int n;                        // window edge (the mixed-size kernels dispatch on it)
+  int skip_band;                // 1: this group leaves out band_columns(n) in every pass
+  TileSkip skip;                // its zero-band tiles (band_tiles), empty when skip_band is 0
 };
 Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                          const float2* tw, cudaStream_t st);
+// Groups of 256^2, 512^2 and 1024^2 windows in one persistent launch (k_row_mixed / k_col_mixed):
+// CTAs of kMixedThreads threads take work units from ``queue`` (an int the caller zeroes) until
+// work_begin[ngroups] units are done; a group has mixed_units(n, row, skip) units per item.
+constexpr int kMixedThreads = 256;
+struct MixedTwiddles {
+  const float2* n256;
+  const float2* n512;
+  const float2* n1024;
+};
+bool mixed_window_ok(int n);
+int mixed_units(int n, bool row, TileSkip skip);
+Status launch_mixed_groups(bool row, const GroupDesc* groups, const int* work_begin, int ngroups, long units,
+                           int tick, const MixedTwiddles& tw, int* queue, cudaStream_t st);
 // ``skip``: column tiles left out of the launch, wholly inside the zero band of every group in it
 Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                          const float2* tw, TileSkip skip, cudaStream_t st);

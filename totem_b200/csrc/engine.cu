@@ -9,8 +9,12 @@
 //  * probes run in batches sized for the L2 cache instead of for half the free memory
 //    (cuda_source_lobato.cu:1250);
 //  * every CUDA / cuFFT status is checked and returned as a TOTEM_ERR_* code.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <atomic>
+#include <cctype>
+#include <fstream>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -44,6 +48,94 @@ std::atomic<size_t> g_tx_scratch{0};
 int fail(const Status& s) {
   g_last_error = s.msg;
   return s.code;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tuning table: launch shapes per (GPU name, window edge), measured by python -m totem_b200.tune
+// ---------------------------------------------------------------------------------------------
+struct TuneEntry {
+  std::string device;
+  int n = 0;
+  int row_variant = 0, col_variant = 0;
+  long long batch_bytes = 0;
+};
+std::mutex g_tune_mu;
+bool g_tune_loaded = false;
+std::vector<TuneEntry> g_tune;
+
+// The value of "key" in one line of the table (a flat JSON object of numbers and strings).
+bool json_field(const std::string& line, const char* key, std::string* out) {
+  const std::string k = std::string("\"") + key + "\"";
+  size_t p = line.find(k);
+  if (p == std::string::npos) return false;
+  p = line.find(':', p + k.size());
+  if (p == std::string::npos) return false;
+  ++p;
+  while (p < line.size() && std::isspace((unsigned char)line[p])) ++p;
+  if (p < line.size() && line[p] == '"') {
+    const size_t e = line.find('"', p + 1);
+    if (e == std::string::npos) return false;
+    *out = line.substr(p + 1, e - p - 1);
+    return true;
+  }
+  size_t e = p;
+  while (e < line.size() && line[e] != ',' && line[e] != '}' && !std::isspace((unsigned char)line[e])) ++e;
+  *out = line.substr(p, e - p);
+  return !out->empty();
+}
+
+Status read_tuning(const std::string& path, std::vector<TuneEntry>* out) {
+  std::ifstream f(path);
+  if (!f) return Status::Err(TOTEM_ERR_INVALID_ARG, "cannot open the tuning table " + path);
+  std::string line, v;
+  int lineno = 0;
+  while (std::getline(f, line)) {
+    ++lineno;
+    if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+    TuneEntry e;
+    if (!json_field(line, "device", &e.device) || !json_field(line, "n", &v))
+      return Status::Err(TOTEM_ERR_INVALID_ARG, path + ":" + std::to_string(lineno) + ": no \"device\" or \"n\"");
+    e.n = std::atoi(v.c_str());
+    if (json_field(line, "row_variant", &v)) e.row_variant = std::atoi(v.c_str());
+    if (json_field(line, "col_variant", &v)) e.col_variant = std::atoi(v.c_str());
+    if (json_field(line, "batch_mib", &v)) e.batch_bytes = (long long)(std::atof(v.c_str()) * 1048576.0);
+    if (e.n <= 0 || e.row_variant < 0 || e.col_variant < 0 || e.batch_bytes < 0)
+      return Status::Err(TOTEM_ERR_INVALID_ARG, path + ":" + std::to_string(lineno) + ": invalid entry");
+    out->push_back(e);
+  }
+  return Status::Ok();
+}
+
+// TOTEM_TUNING_FILE, else data/tuning.jsonl beside the directory this library was loaded from.
+std::string default_tuning_path() {
+  if (const char* e = std::getenv("TOTEM_TUNING_FILE")) return e;
+  Dl_info info;
+  if (dladdr(reinterpret_cast<void*>(&default_tuning_path), &info) && info.dli_fname) {
+    std::string lib(info.dli_fname);
+    const size_t slash = lib.rfind('/');
+    return (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/../data/tuning.jsonl";
+  }
+  return "";
+}
+
+// Entry for (device, n); the default table is read on first use (missing or unreadable: none).
+bool tuned_entry(int device, int n, TuneEntry* out) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (!g_tune_loaded) {
+    g_tune_loaded = true;
+    std::vector<TuneEntry> t;
+    const std::string path = default_tuning_path();
+    if (!path.empty() && read_tuning(path, &t).ok()) g_tune = std::move(t);
+  }
+  if (g_tune.empty()) return false;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return false;
+  for (const TuneEntry& e : g_tune)
+    if (e.n == n && e.device == prop.name) {
+      *out = e;
+      return true;
+    }
+  return false;
 }
 
 // Per-slice counts -> prefix offsets; validates that the counts are whole, non-negative numbers.
@@ -310,7 +402,7 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
     for (size_t i = 0; i < vol; ++i) hp[i] = make_float2((float)a->prop_re[i], (float)a->prop_im[i]);
     TOTEM_TRY(upload(probe, pr, st));
     TOTEM_TRY(upload(prop, hp, st));
-    band = (h == w) ? totem::spectral_band(a->prop_re, a->prop_im, h, w) : totem::kNoBand;
+    band = (h == w) ? totem::spectral_band(a->prop_re, a->prop_im, h, w) : (1 << 30);
     // exit detector: ifftshift(aper) (the reference shifts the wave instead, cuda_source_lobato.cu:1415)
     std::vector<float> me(vol * std::max(aper_num, 1)), mm;
     for (int q = 0; q < aper_num; ++q)
@@ -507,7 +599,7 @@ Status totem_session::transmission_for(int t_storage, const void** t, size_t* sl
 }
 
 Status totem_session::slice_loop(int path, int batch, int col_variant, int t_storage, int* launches,
-                                 int* batch_used) {
+                                 int* batch_used, int row_variant) {
   const long items_total = (long)w_num * depth;
   const long ad = (long)aper_num * depth;
   const int L = (int)mid_layer.size();
@@ -542,9 +634,11 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   }
   *batch_used = B;
   const int nblk = fused ? totem::col_blocks(h, col_variant) : 64;
-  // the zero band of the propagator: columns the fused passes skip, tiles the detector sums skip
-  const int band_run = (fused && totem::band_skip_enabled()) ? band : totem::kNoBand;
-  const totem::TileSkip skip = fused ? totem::zero_tiles(h, nblk, band_run) : totem::TileSkip();
+  // the zero band of the propagator: columns the fused passes leave out, tiles the detector sums
+  // leave out (the bfloat16 trial computes every column)
+  const bool skip_band = fused && totem::band_skip_enabled() && t_storage == TOTEM_T_COMPLEX64 &&
+                         totem::band_skip_ok(h, band, col_variant);
+  const totem::TileSkip skip = skip_band ? totem::band_tiles(h, nblk) : totem::TileSkip();
   TOTEM_TRY(psi.ensure((size_t)B * vol * sizeof(float2)));
   TOTEM_TRY(part.ensure((size_t)n_events * B * aper_num * nblk * sizeof(double)));
   TOTEM_TRY(acc.ensure((size_t)n_events * w_num * ad * sizeof(double)));
@@ -575,7 +669,8 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
         s.mask_mid = mask_mid.as<float>(); s.mask_exit = mask_exit.as<float>();
         s.col_variant = col_variant;
         s.t_bf16 = (t_storage == TOTEM_T_BF16);
-        s.band = band_run;
+        s.skip_band = skip_band ? 1 : 0;
+        s.row_variant = row_variant;
         TOTEM_TRY(prof_begin());
         TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
         TOTEM_TRY(prof_end(0));
@@ -643,7 +738,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
     // what the launches embed: sizes, buffer addresses and the detection events
     std::vector<long long> key = {h, items_total, B, slices, col_variant, t_storage, n_events, exit_event, aper_num,
                                   w_num, depth, nblk, L, p_h, p_w, begin_row, begin_col, step, width_red,
-                                  (long long)tslice_bytes, band_run};
+                                  (long long)tslice_bytes, skip_band ? 1 : 0, row_variant};
     for (const void* q : {(const void*)psi.p, (const void*)part.p, (const void*)acc.p, (const void*)probe.p,
                           (const void*)prop.p, (const void*)tw_n.p, (const void*)mask_mid.p, (const void*)mask_exit.p,
                           Tslices, (const void*)gfsf_d.p, (const void*)out_result.p, (const void*)out_mid.p})
@@ -782,7 +877,12 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
   s.tw = tw_pw.as<float2>();
   s.aper_num = 0;
   s.t_bf16 = (hr->t_storage == TOTEM_T_BF16);
-  s.band = totem::band_skip_enabled() ? totem::spectral_band(hr->prop_re, hr->prop_im, n, n) : totem::kNoBand;
+  // every pass leaves out the propagator's zero band (the last column pass writes zeros there
+  // into the kept spectrum); the bfloat16 trial computes every column
+  s.skip_band = (totem::band_skip_enabled() && hr->t_storage == TOTEM_T_COMPLEX64 &&
+                 totem::band_skip_ok(n, totem::spectral_band(hr->prop_re, hr->prop_im, n, n), 0))
+                    ? 1
+                    : 0;
   auto tslice = [&](int k) { return static_cast<const char*>(Tslices) + (size_t)k * tslice_bytes; };
   // psi = wave .* T_0, then per slice FFT2 .* psf_fft IFFT2 .* T_{k+1}; the last column pass keeps
   // the spectrum FFT2(psi_{S-1} .* T) .* psf_fft, whose IFFT2 is the exit wave
@@ -848,7 +948,20 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
     if (!stem_ready && depth > 0) return Status::Err(TOTEM_ERR_STATE, "no STEM inputs uploaded");
     if (o.t_storage != TOTEM_T_COMPLEX64 && o.t_storage != TOTEM_T_BF16)
       return Status::Err(TOTEM_ERR_INVALID_ARG, "unknown transmission storage");
-    TOTEM_TRY(slice_loop(o.path, o.batch, o.col_variant, o.t_storage, &launches, &batch_used));
+    // launch shapes left at 0: the tuning table's entry for this GPU and window, else built-in
+    int rv = o.row_variant, cv = o.col_variant, batch = o.batch;
+    if (o.path != TOTEM_PATH_PLAIN && h == w && (rv == 0 || cv == 0 || batch == 0)) {
+      TuneEntry e;
+      if (tuned_entry(device, h, &e)) {
+        if (rv == 0) rv = e.row_variant;
+        if (cv == 0) cv = e.col_variant;
+        if (batch == 0 && e.batch_bytes > 0)
+          batch = (int)std::max<long long>(1, e.batch_bytes / ((long long)h * w * (long long)sizeof(float2)));
+      }
+    }
+    used_row_variant = rv ? rv : 1;
+    used_col_variant = cv ? cv : 1;
+    TOTEM_TRY(slice_loop(o.path, batch, cv, o.t_storage, &launches, &batch_used, rv));
   }
   else has_result = true;
   TOTEM_CUDA(cudaEventRecord(ev[2], stream));
@@ -861,6 +974,8 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
   timing.slice_path = ran_slice_path;
   timing.tx_fft_path = ran_tx_fft;
   timing.tx_builder = ran_tx_builder;
+  timing.row_variant = (what == 0 && ran_slice_path == TOTEM_PATH_FUSED) ? used_row_variant : 0;
+  timing.col_variant = (what == 0 && ran_slice_path == TOTEM_PATH_FUSED) ? used_col_variant : 0;
   timing_pending = true;
   return Status::Ok();
 }
@@ -1119,6 +1234,36 @@ int totem_set_slice_graphs(int enable) {
   g_slice_graphs.store(enable);
   g_last_error.clear();
   return TOTEM_OK;
+}
+
+int totem_load_tuning(const char* path, int* entries) {
+  return guarded([&]() -> Status {
+    std::vector<TuneEntry> t;
+    if (path && *path) TOTEM_TRY(read_tuning(path, &t));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune = std::move(t);
+    g_tune_loaded = true;
+    if (entries) *entries = (int)g_tune.size();
+    return Status::Ok();
+  });
+}
+
+int totem_tuned_config(int device, int n, int* row_variant, int* col_variant, long long* batch_bytes) {
+  if (!row_variant || !col_variant || !batch_bytes || n <= 0)
+    return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "invalid tuned-config arguments"));
+  return guarded([&]() -> Status {
+    TOTEM_TRY(totem::pick_device(&device));
+    *row_variant = 1;
+    *col_variant = 1;
+    *batch_bytes = 4ll << 30;
+    TuneEntry e;
+    if (tuned_entry(device, n, &e)) {
+      if (e.row_variant) *row_variant = e.row_variant;
+      if (e.col_variant) *col_variant = e.col_variant;
+      if (e.batch_bytes) *batch_bytes = e.batch_bytes;
+    }
+    return Status::Ok();
+  });
 }
 
 int totem_set_band_skip(int enable) {

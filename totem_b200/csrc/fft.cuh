@@ -433,7 +433,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Launch shapes shared by the kernels that transform whole rows or whole columns.
 // Rows: G transforms of T threads per CTA (each transform inside one warp, or a named barrier
 // per transform when T > 32), at most 32 KB of exchange space per CTA.
-template <int N>
+template <int N, int CTAS = 0>
 struct RowCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
   static constexpr int G = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
@@ -443,7 +443,8 @@ struct RowCfg {
   // row pass 12 % faster (3.51 against 4.01 us per probe; no change at 512); from N = 2048
   // (three-stage transforms) 3, i.e. ~170 registers: the 2048 row pass spilled 200 B at 128
   // and ran 22 % slower
-  static constexpr int CTAS128 = (N <= 512) ? 5 : (N <= 1024 ? 4 : 3);
+  // CTAS != 0 (a row-pass variant) replaces the default
+  static constexpr int CTAS128 = CTAS ? CTAS : ((N <= 512) ? 5 : (N <= 1024 ? 4 : 3));
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };
 // Columns: G adjacent columns per CTA, thread (j, g) = (tid / G, tid % G), so a warp's loads
@@ -456,6 +457,22 @@ struct ColCfg {
   static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 2048 ? 8 : 2));
   // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
+};
+
+constexpr int gcd_c(int a, int b) { return b ? gcd_c(b, a % b) : a; }
+// Columns [lo, hi) of an N x N window that lie beyond the reference's 2/3-of-Nyquist propagator
+// cut (index distance from DC above N / 3, ToTEM_submit_v1.m:1558-1564), rounded inward to whole
+// groups of T row-pass elements and whole default column tiles.  When the propagator is zero on
+// them (checked per request), every column pass turns them into zeros, so the row pass neither
+// loads nor stores them (a compile-time choice: those loads and stores are not emitted) and the
+// column pass leaves their tiles out (lo = hi: nothing to leave out).
+template <int N>
+struct BandCols {
+  static constexpr int T = Fft<N>::T, G = ColCfg<N>::G;
+  static constexpr int L = T / gcd_c(T, G) * G;
+  static constexpr int K = N / 3;
+  static constexpr int lo = (K + 1 + L - 1) / L * L;
+  static constexpr int hi = ((N - K) / L * L > lo) ? (N - K) / L * L : lo;
 };
 
 template <int N>

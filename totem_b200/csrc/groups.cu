@@ -1,0 +1,193 @@
+// Continuous batching: row and column passes over groups of items of several requests, each
+// group at its own slice; per window size, or (mixed) over 256^2 .. 1024^2 windows at once.
+#include "slice_tiles.cuh"
+
+namespace totem {
+
+namespace {
+
+// Row pass of a continuous batch over groups of one window size.
+template <int N>
+__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
+    k_row_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
+                 const float2* __restrict__ tw) {
+  constexpr int G = RowCfg<N>::G, per_item = N / G;
+  const int li = blockIdx.x / per_item;
+  const int row0 = (blockIdx.x - li * per_item) * G;
+  const int gidx = find_group(item_begin, ngroups, li);
+  row_group_tile<N>(groups[gidx], li - __ldg(item_begin + gidx), row0, tick, tw);
+}
+
+// Column pass of a continuous batch over groups of one window size.
+template <int N>
+__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB)
+    k_col_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
+                 const float2* __restrict__ tw, TileSkip skip) {
+  constexpr int G = ColCfg<N>::G, nblk = N / G;
+  const int active = nblk - skip.nskip;
+  const int li = blockIdx.x / active, t = blockIdx.x - li * active;
+  const int cb = t < skip.z0 ? t : t + skip.nskip;
+  const int gidx = find_group(item_begin, ngroups, li);
+  col_group_tile<N, G>(groups[gidx], li - __ldg(item_begin + gidx), cb, tick, tw);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Windows of different sizes in one launch.  A persistent CTA of kMixedThreads threads takes
+// work units from a queue (an atomic counter) until the launch's units run out; a unit is
+// kMixedThreads / T rows (row pass) or one column tile (column pass, the tile width of the
+// single-size kernel, so the detector partial sums are the same) of one item of one group,
+// groups of 256^2, 512^2 and 1024^2 windows mixed.  The per-tile code is the single-size
+// kernels', so every result is bit-identical to the per-size launches.  Units are numbered group
+// by group: work_begin[g] is the first unit of group g, work_begin[ngroups] the total.
+// ---------------------------------------------------------------------------------------------
+template <int N>
+constexpr int mixed_row_units() { return N / (kMixedThreads / Fft<N>::T); }
+
+__device__ __forceinline__ int take_unit(int* queue) {
+  __shared__ int s_unit;
+  __syncthreads();  // the previous unit is done with shared memory
+  if (threadIdx.x == 0) s_unit = atomicAdd(queue, 1);
+  __syncthreads();
+  return s_unit;
+}
+
+__global__ void __launch_bounds__(kMixedThreads, 2)
+    k_row_mixed(const GroupDesc* __restrict__ groups, const int* __restrict__ work_begin, int ngroups, int tick,
+                MixedTwiddles tw, int* queue) {
+  const int total = __ldg(work_begin + ngroups);
+  for (int u = take_unit(queue); u < total; u = take_unit(queue)) {
+    const int gidx = find_group(work_begin, ngroups, u);
+    const GroupDesc& d = groups[gidx];
+    const int lu = u - __ldg(work_begin + gidx);
+    switch (d.n) {
+#define TOTEM_ROW_MIXED(NN, TW)                                                                   \
+  case NN: {                                                                                      \
+    constexpr int rows = kMixedThreads / Fft<NN>::T, per_item = NN / rows;                        \
+    row_group_tile<NN>(d, lu / per_item, (lu % per_item) * rows, tick, tw.TW);                    \
+    break;                                                                                        \
+  }
+      TOTEM_ROW_MIXED(256, n256) TOTEM_ROW_MIXED(512, n512) TOTEM_ROW_MIXED(1024, n1024)
+#undef TOTEM_ROW_MIXED
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kMixedThreads, 2)
+    k_col_mixed(const GroupDesc* __restrict__ groups, const int* __restrict__ work_begin, int ngroups, int tick,
+                MixedTwiddles tw, int* queue) {
+  const int total = __ldg(work_begin + ngroups);
+  for (int u = take_unit(queue); u < total; u = take_unit(queue)) {
+    const int gidx = find_group(work_begin, ngroups, u);
+    const GroupDesc& d = groups[gidx];
+    const int lu = u - __ldg(work_begin + gidx);
+    switch (d.n) {
+#define TOTEM_COL_MIXED(NN, TW)                                                                   \
+  case NN: {                                                                                      \
+    constexpr int G = ColCfg<NN>::G;                                                              \
+    static_assert(G * ColCfg<NN>::T == kMixedThreads, "mixed column tiles use the single-size tile width"); \
+    const int active = NN / G - d.skip.nskip;                                                     \
+    const int t = lu % active;                                                                    \
+    col_group_tile<NN, G>(d, lu / active, t < d.skip.z0 ? t : t + d.skip.nskip, tick, tw.TW);     \
+    break;                                                                                        \
+  }
+      TOTEM_COL_MIXED(256, n256) TOTEM_COL_MIXED(512, n512) TOTEM_COL_MIXED(1024, n1024)
+#undef TOTEM_COL_MIXED
+    }
+  }
+}
+
+}  // namespace
+
+template <int N>
+Status row_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
+                  cudaStream_t st) {
+  constexpr int G = RowCfg<N>::G, T = RowCfg<N>::T;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_row_groups<N>, smem));
+  k_row_groups<N><<<(unsigned)(items * (N / G)), G * T, smem, st>>>(groups, item_begin, ngroups, tick, tw);
+  return cuda_status(cudaGetLastError(), "k_row_groups");
+}
+
+template <int N>
+Status col_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
+                  TileSkip skip, cudaStream_t st) {
+  constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_col_groups<N>, smem));
+  if (skip.nskip < 0 || skip.z0 < 0 || skip.z0 + skip.nskip > N / G)
+    return Status::Err(TOTEM_ERR_STATE, "column tiles to skip out of range");
+  k_col_groups<N><<<(unsigned)(items * (N / G - skip.nskip)), G * T, smem, st>>>(groups, item_begin, ngroups, tick,
+                                                                                 tw, skip);
+  return cuda_status(cudaGetLastError(), "k_col_groups");
+}
+
+Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                         const float2* tw, cudaStream_t st) {
+  if (items <= 0 || ngroups <= 0) return Status::Ok();
+  switch (n) {
+    case 64: return row_groups<64>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 128: return row_groups<128>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 256: return row_groups<256>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 512: return row_groups<512>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 1024: return row_groups<1024>(groups, item_begin, ngroups, items, tick, tw, st);
+    case 2048: return row_groups<2048>(groups, item_begin, ngroups, items, tick, tw, st);
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
+}
+
+Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                         const float2* tw, TileSkip skip, cudaStream_t st) {
+  if (items <= 0 || ngroups <= 0) return Status::Ok();
+  switch (n) {
+    case 64: return col_groups<64>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 128: return col_groups<128>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 256: return col_groups<256>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 512: return col_groups<512>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 1024: return col_groups<1024>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+    case 2048: return col_groups<2048>(groups, item_begin, ngroups, items, tick, tw, skip, st);
+  }
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
+}
+
+template <int N>
+size_t mixed_smem() {
+  constexpr int rows = kMixedThreads / Fft<N>::T;
+  const size_t row = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(rows));
+  const size_t col = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, ColCfg<N>::G>::size(ColCfg<N>::G));
+  return row > col ? row : col;
+}
+
+int mixed_units(int n, bool row, TileSkip skip) {
+  switch (n) {
+    case 256: return row ? mixed_row_units<256>() : 256 / ColCfg<256>::G - skip.nskip;
+    case 512: return row ? mixed_row_units<512>() : 512 / ColCfg<512>::G - skip.nskip;
+    case 1024: return row ? mixed_row_units<1024>() : 1024 / ColCfg<1024>::G - skip.nskip;
+  }
+  return 0;
+}
+
+bool mixed_window_ok(int n) { return n == 256 || n == 512 || n == 1024; }
+
+Status launch_mixed_groups(bool row, const GroupDesc* groups, const int* work_begin, int ngroups, long units,
+                           int tick, const MixedTwiddles& tw, int* queue, cudaStream_t st) {
+  if (units <= 0 || ngroups <= 0) return Status::Ok();
+  size_t smem = mixed_smem<256>();
+  smem = std::max(smem, mixed_smem<512>());
+  smem = std::max(smem, mixed_smem<1024>());
+  const void* fn = row ? (const void*)k_row_mixed : (const void*)k_col_mixed;
+  TOTEM_TRY(ensure_smem(fn, smem));
+  static int ctas = 0;  // resident CTAs of the whole GPU (both kernels: same shape and bounds)
+  if (ctas == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    TOTEM_CUDA(cudaGetDevice(&dev));
+    TOTEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    TOTEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_row_mixed, kMixedThreads, smem));
+    ctas = std::max(1, sms * std::max(per_sm, 1));
+  }
+  const unsigned grid = (unsigned)std::min<long>(units, ctas);
+  if (row) k_row_mixed<<<grid, kMixedThreads, smem, st>>>(groups, work_begin, ngroups, tick, tw, queue);
+  else k_col_mixed<<<grid, kMixedThreads, smem, st>>>(groups, work_begin, ngroups, tick, tw, queue);
+  return cuda_status(cudaGetLastError(), row ? "k_row_mixed" : "k_col_mixed");
+}
+
+}  // namespace totem

@@ -57,7 +57,7 @@ struct Request {
   totem::DetectionEvents de;
   long long items = 0, items_left = 0;
   int nblk = 0;
-  int band = totem::kNoBand;        // zero band of the request's propagator used by its launches
+  int skip_band = 0;                // its groups leave out the propagator's zero band
   size_t item_bytes = 0;
   long long probe_slices = 0;
   double est = 0;                   // estimated device seconds (preparation order)
@@ -173,7 +173,9 @@ Status totem_server::init() {
   if (!opt.chunk_bytes) opt.chunk_bytes = wave / 4;
   static_budget = budget - wave;
   K = opt.ticks_ahead > 0 ? opt.ticks_ahead : 4;
-  slot_bytes = max_groups * (sizeof(totem::GroupDesc) + sizeof(int)) + 64 * (sizeof(int) + 256);
+  // per window size: descriptors, launch-item prefix, alignment; the mixed launch adds a second
+  // prefix and two queue counters
+  slot_bytes = max_groups * (sizeof(totem::GroupDesc) + 2 * sizeof(int)) + 64 * (sizeof(int) + 256) + 1024;
   // Tick streams run above the default priority of the preparation streams, so slice steps of
   // running requests are not queued behind transmission builds; the fast lane above the bulk lane.
   int least = 0, greatest = 0;
@@ -247,7 +249,7 @@ Status totem_server::prepare(Request* r) {
   r->items = (s->aper_num > 0) ? (long long)s->w_num * s->depth : 0;
   r->items_left = r->items;
   r->nblk = totem::col_blocks(s->h);
-  r->band = totem::band_skip_enabled() ? s->band : totem::kNoBand;
+  r->skip_band = (totem::band_skip_enabled() && totem::band_skip_ok(s->h, s->band, 0)) ? 1 : 0;
   r->item_bytes = (size_t)s->h * s->w * sizeof(float2) + (size_t)r->de.n_events * s->aper_num * r->nblk * sizeof(double);
   r->probe_slices = (long long)s->w_num * s->depth * s->slices;
   TOTEM_CUDA(cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming));
@@ -362,15 +364,96 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
   char* h = lane.h_stage + (size_t)slot * slot_bytes;
   char* d = lane.d_stage + (size_t)slot * slot_bytes;
   size_t off = 0;
-  for (auto& kv : by_n) {
-    const int n = kv.first;
-    const std::vector<const totem::PlanGroup*>& gs = kv.second;
+  auto twiddles_of = [&](int n, const float2** out) -> Status {
     auto& twb = tw[n];
     if (!twb) {
       twb.reset(new totem::DevBuf());
       TOTEM_TRY(totem::upload(*twb, totem::twiddles(n), sst));
       TOTEM_CUDA(cudaStreamSynchronize(sst));  // once per window size: the other lane may use it next
     }
+    *out = twb->as<float2>();
+    return Status::Ok();
+  };
+  auto describe = [&](const totem::PlanGroup& g, int n, totem::GroupDesc& x) -> Status {
+    Request* r = nullptr;
+    TOTEM_TRY(lookup(g.req, &r));
+    const totem_session* s = r->sess;
+    x.psi = static_cast<float2*>(g.psi);
+    x.t_stack = s->T.as<float2>();
+    x.probe = s->probe.as<float2>();
+    x.prop = s->prop.as<float2>();
+    x.mask_mid = s->mask_mid.as<float>();
+    x.mask_exit = s->mask_exit.as<float>();
+    x.part = static_cast<double*>(g.part);
+    x.event_of_slice = s->ev_slice.as<int>();
+    x.geo = totem::ScanGeom{s->begin_row, s->begin_col, s->step, s->width_red, s->depth, s->p_w};
+    x.p_h = s->p_h;
+    x.item0 = (int)g.item0;
+    x.items = g.items;
+    x.start_tick = g.start_tick;
+    x.slices = s->slices;
+    x.aper_num = s->aper_num;
+    x.exit_event = r->de.exit_event;
+    x.n = n;
+    x.skip_band = r->skip_band;
+    x.skip = r->skip_band ? totem::band_tiles(n, totem::col_blocks(n)) : totem::TileSkip();
+    return Status::Ok();
+  };
+  // Several of the window sizes 256^2 .. 1024^2 at this tick: one persistent launch per pass for
+  // all of them (TotemServerOptions.mixed_windows)
+  int mixed_sizes = 0;
+  for (auto& kv : by_n) mixed_sizes += totem::mixed_window_ok(kv.first) ? 1 : 0;
+  if (opt.mixed_windows == 1 && mixed_sizes >= 2) {
+    std::vector<const totem::PlanGroup*> gs;
+    totem::MixedTwiddles mt{nullptr, nullptr, nullptr};
+    for (auto it = by_n.begin(); it != by_n.end();) {
+      if (!totem::mixed_window_ok(it->first)) {
+        ++it;
+        continue;
+      }
+      const float2* t = nullptr;
+      TOTEM_TRY(twiddles_of(it->first, &t));
+      (it->first == 256 ? mt.n256 : it->first == 512 ? mt.n512 : mt.n1024) = t;
+      gs.insert(gs.end(), it->second.begin(), it->second.end());
+      it = by_n.erase(it);
+    }
+    const size_t ng = gs.size();
+    const size_t desc_off = off, rb_off = off + ng * sizeof(totem::GroupDesc), cb_off = rb_off + (ng + 1) * sizeof(int);
+    const size_t q_off = cb_off + (ng + 1) * sizeof(int);
+    off = q_off + 2 * sizeof(int);
+    off = (off + 255) & ~(size_t)255;
+    if (off > slot_bytes) return Status::Err(TOTEM_ERR_STATE, "scheduler staging slot overflow");
+    auto* desc = reinterpret_cast<totem::GroupDesc*>(h + desc_off);
+    auto* rb = reinterpret_cast<int*>(h + rb_off);
+    auto* cbg = reinterpret_cast<int*>(h + cb_off);
+    auto* q = reinterpret_cast<int*>(h + q_off);
+    long long row_units = 0, col_units = 0;
+    for (size_t i = 0; i < ng; ++i) {
+      TOTEM_TRY(describe(*gs[i], gs[i]->n, desc[i]));
+      rb[i] = (int)row_units;
+      cbg[i] = (int)col_units;
+      row_units += (long long)gs[i]->items * totem::mixed_units(gs[i]->n, true, desc[i].skip);
+      col_units += (long long)gs[i]->items * totem::mixed_units(gs[i]->n, false, desc[i].skip);
+    }
+    if (row_units > INT32_MAX || col_units > INT32_MAX)
+      return Status::Err(TOTEM_ERR_STATE, "too many work units in one mixed launch");
+    rb[ng] = (int)row_units;
+    cbg[ng] = (int)col_units;
+    q[0] = q[1] = 0;
+    TOTEM_CUDA(cudaMemcpyAsync(d + desc_off, h + desc_off, off - desc_off, cudaMemcpyHostToDevice, sst));
+    const auto* dd = reinterpret_cast<const totem::GroupDesc*>(d + desc_off);
+    int* dq = reinterpret_cast<int*>(d + q_off);
+    TOTEM_TRY(totem::launch_mixed_groups(true, dd, reinterpret_cast<const int*>(d + rb_off), (int)ng, row_units, tick,
+                                         mt, dq, sst));
+    TOTEM_TRY(totem::launch_mixed_groups(false, dd, reinterpret_cast<const int*>(d + cb_off), (int)ng, col_units,
+                                         tick, mt, dq + 1, sst));
+    launched += 2;
+  }
+  for (auto& kv : by_n) {
+    const int n = kv.first;
+    const std::vector<const totem::PlanGroup*>& gs = kv.second;
+    const float2* twn = nullptr;
+    TOTEM_TRY(twiddles_of(n, &twn));
     const size_t ng = gs.size();
     const size_t desc_off = off, ib_off = off + ng * sizeof(totem::GroupDesc);
     off = ib_off + (ng + 1) * sizeof(int);
@@ -384,30 +467,10 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
     int skip_lo = 0, skip_hi = nblk_n;
     for (size_t i = 0; i < ng; ++i) {
       const totem::PlanGroup& g = *gs[i];
-      Request* r = nullptr;
-      TOTEM_TRY(lookup(g.req, &r));
-      const totem_session* s = r->sess;
       totem::GroupDesc& x = desc[i];
-      x.psi = static_cast<float2*>(g.psi);
-      x.t_stack = s->T.as<float2>();
-      x.probe = s->probe.as<float2>();
-      x.prop = s->prop.as<float2>();
-      x.mask_mid = s->mask_mid.as<float>();
-      x.mask_exit = s->mask_exit.as<float>();
-      x.part = static_cast<double*>(g.part);
-      x.event_of_slice = s->ev_slice.as<int>();
-      x.geo = totem::ScanGeom{s->begin_row, s->begin_col, s->step, s->width_red, s->depth, s->p_w};
-      x.p_h = s->p_h;
-      x.item0 = (int)g.item0;
-      x.items = g.items;
-      x.start_tick = g.start_tick;
-      x.slices = s->slices;
-      x.aper_num = s->aper_num;
-      x.exit_event = r->de.exit_event;
-      x.band = r->band;
-      const totem::TileSkip zt = totem::zero_tiles(n, nblk_n, r->band);
-      skip_lo = std::max(skip_lo, zt.z0);
-      skip_hi = std::min(skip_hi, zt.z0 + zt.nskip);
+      TOTEM_TRY(describe(g, n, x));
+      skip_lo = std::max(skip_lo, x.skip.z0);
+      skip_hi = std::min(skip_hi, x.skip.z0 + x.skip.nskip);
       ib[i] = (int)items;
       items += g.items;
     }
@@ -415,13 +478,13 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
     TOTEM_CUDA(cudaMemcpyAsync(d + desc_off, h + desc_off, off - desc_off, cudaMemcpyHostToDevice, sst));
     const auto* dd = reinterpret_cast<const totem::GroupDesc*>(d + desc_off);
     const auto* dib = reinterpret_cast<const int*>(d + ib_off);
-    TOTEM_TRY(totem::launch_row_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), sst));
+    TOTEM_TRY(totem::launch_row_groups(n, dd, dib, (int)ng, items, tick, twn, sst));
     totem::TileSkip skip;
     if (skip_hi > skip_lo) {
       skip.z0 = skip_lo;
       skip.nskip = skip_hi - skip_lo;
     }
-    TOTEM_TRY(totem::launch_col_groups(n, dd, dib, (int)ng, items, tick, twb->as<float2>(), skip, sst));
+    TOTEM_TRY(totem::launch_col_groups(n, dd, dib, (int)ng, items, tick, twn, skip, sst));
     launched += 2;
   }
   // groups that ran their last slice: detector sums, then their wave memory goes back
@@ -435,7 +498,7 @@ Status totem_server::tick_once(Lane& lane, bool* progressed) {
       TOTEM_TRY(totem::launch_det_reduce(static_cast<const double*>(g.part) + e * estride, r->nblk, s->aper_num,
                                          g.items, (int)g.item0, s->depth,
                                          s->acc.as<double>() + (size_t)e * s->w_num * ad, sst,
-                                         totem::zero_tiles(s->h, r->nblk, r->band)));
+                                         r->skip_band ? totem::band_tiles(s->h, r->nblk) : totem::TileSkip()));
     launched += r->de.n_events;
     TOTEM_CUDA(cudaFreeAsync(g.psi, sst));
     TOTEM_CUDA(cudaFreeAsync(g.part, sst));

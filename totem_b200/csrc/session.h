@@ -193,10 +193,11 @@ struct totem_session {
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   TotemTiming timing{};
   long long h2d_bytes = 0, d2h_bytes = 0;
-  // zero band of the uploaded propagator (totem::spectral_band), kNoBand if none is known
-  int band = totem::kNoBand;
+  // band of the uploaded propagator (totem::spectral_band; n / 2 and above: no zero band)
+  int band = 1 << 30;
   // which implementations the last run used (TotemTiming.slice_path / tx_fft_path / tx_builder)
   int ran_slice_path = -1, ran_tx_fft = -1, ran_tx_builder = -1;
+  int used_row_variant = 0, used_col_variant = 0;
   // per-launch profiling of the fused passes (TotemRunOptions.profile)
   bool profiling = false;
   std::vector<cudaEvent_t> pev;
@@ -279,7 +280,8 @@ struct totem_session {
   // Per-event detector sums acc[event][w][A][depth] -> out_result (exit) and out_mid (layers),
   // weighted by gfsf over w (accumulate_result, cuda_source_lobato.cu:981-1015).
   Status combine_results(const totem::DetectionEvents& de, int* launches);
-  Status slice_loop(int path, int batch, int col_variant, int t_storage, int* launches, int* batch_used);
+  Status slice_loop(int path, int batch, int col_variant, int t_storage, int* launches, int* batch_used,
+                    int row_variant = 0);
   // The transmission slices as the slice loop reads them (complex64, or bfloat16 pairs).
   Status transmission_for(int t_storage, const void** t, size_t* slice_bytes, int* launches);
   Status run_graphed(const std::vector<long long>& key, const std::function<Status()>& enqueue, int* launches);
