@@ -64,7 +64,9 @@ def test_gridding_ionic_absorptive_and_vacuum_slices(engine_lib):
 
 
 def test_correction_rows_both_builders(engine_lib):
-    # Peng-extended correction rows (per-pixel planes) added after either builder's species sums
+    # Peng-extended correction rows (per-pixel planes) summed by species in either builder: the
+    # structure factor of each group of identical correction rows times its amplitude, Debye-Waller
+    # envelope and plane(s); and on a non-separable grid by the per-atom kernel
     req = request.with_correction(request.build_small_stem(flag="p"))
     ref = so.transmission(req)
     assert rel_l2(ref, so.transmission(replace(req, corr_info_matrix=None))) > 10 * TOL  # rows matter
@@ -135,3 +137,19 @@ def test_gridding_stem_vs_direct_1024(engine_lib):
     for a in range(A):
         assert rel_l2(rg.reshape(A, D)[a], rd.reshape(A, D)[a]) < 1e-5
 
+
+
+def test_correction_rows_on_a_non_separable_grid(engine_lib):
+    # a reciprocal grid that is not a meshgrid (kx depending on the row) takes the per-atom kernel
+    # for every kind of row, the correction rows included
+    req = request.with_correction(request.build_small_stem(flag="p", slices=3))
+    kx = req.kx.copy()
+    kx[1::2] *= 1.0 + 1e-9  # breaks the separable layout, changes the physics negligibly
+    bent = replace(req, kx=kx)
+    s = capi.Session()
+    s.upload(bent)
+    s.run(what=1)
+    assert s.timing().tx_builder == capi.TX_ROWS
+    t = s.download(want_transmission=True)[2]
+    s.close()
+    assert rel_l2(t, so.transmission(bent)) < TOL

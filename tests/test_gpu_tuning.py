@@ -41,8 +41,9 @@ def test_tuned_pick_within_3_percent_of_best_hand_configuration(engine_lib, n):
 def test_engine_applies_the_table(engine_lib, tmp_path):
     req = request.build_small_stem(raster=(3, 3))
     path = tmp_path / "t.jsonl"
+    # 1/16 MiB of waves: two 64^2 probes per batch (the 9 probes run in 5 batches of at most 2)
     path.write_text(json.dumps({"device": tune.device_name(0), "n": req.height, "row_variant": 4, "col_variant": 5,
-                                "batch_mib": 1}) + "\n")
+                                "batch_mib": 0.0625}) + "\n")
     try:
         assert capi.load_tuning(str(path)) == 1
         s = capi.Session(device=0)
@@ -51,7 +52,7 @@ def test_engine_applies_the_table(engine_lib, tmp_path):
         res, mid, _ = s.download()
         t = s.timing()
         assert (t.row_variant, t.col_variant) == (4, 5)
-        assert t.batch == max(1, (1 << 20) // (req.height * req.width * 8))
+        assert t.batch == 2
         s.run(col_variant=1, batch=9)  # explicit options win
         t = s.timing()
         assert (t.row_variant, t.col_variant, t.batch) == (4, 1, 9)

@@ -90,16 +90,21 @@ struct SpeciesDev {
   int ncoef = 0;
 };
 
+// The four kinds of coefficient rows by species: 0 neutral, 1 ionic, 2 Peng-extended correction
+// (neutral, [B, amplitude, plane]), 3 correction (ionic, [B, amplitude, w1, plane1, w2, plane2]).
+struct SpeciesSet {
+  SpeciesDev k[4];
+};
+
 // V_k(g) * PARAMETER * APERTURE for all slices into out[slice][p_h][p_w] (complex64), one
 // thread per pixel and atom row.  accumulate: add to out instead of overwriting it.
 Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const AtomRowsDev& ion,
                            const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out,
                            cudaStream_t st, bool accumulate = false);
-// The neutral and ionic terms of the same sum on separable grids, by species: a complex rank-K
-// update per species (no exponential per atom and pixel), then the form factor once per species
-// and pixel.  Overwrites out.
-Status launch_tx_species(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, float2* out,
-                         cudaStream_t st);
+// The same sums on separable grids, by species (all four kinds): a complex rank-K update per
+// species (no exponential per atom and pixel), then the form factor once per species and pixel.
+// Overwrites out.
+Status launch_tx_species(const TxGrid& g, const SpeciesSet& sp, float2* out, cudaStream_t st);
 // The same sums by Gaussian gridding (a type-1 non-uniform FFT) on uniform separable grids.
 // Work is grouped in jobs, one per (slice, kind, species) segment, ordered by slice; a batch
 // runs the jobs [j_lo, j_hi) in scratch memory and writes slices [s_lo, s_hi) (the last may be
@@ -109,7 +114,7 @@ struct GridPlanDev {
   double sx = 0, sy = 0;           // kx(p_w / 2), ky(p_h / 2): the shift folded into each atom's weight
   const float2* ax = nullptr;      // [p_w][2]: Gaussian deconvolution x half-bin phase (parity 0, 1)
   const float2* ay = nullptr;      // [p_h][2]
-  const int4* jobs = nullptr;      // [jobs]: kind, species, first atom, end atom
+  const int4* jobs = nullptr;      // [jobs]: kind (SpeciesSet index), species, first atom, end atom
   const int* job_beg = nullptr;    // [slices + 1] first job of every slice
 };
 struct GridBatch {
@@ -120,7 +125,7 @@ std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_pe
 inline size_t grid_job_bytes(int p_h, int p_w) { return (size_t)p_h * p_w * 64 + (size_t)p_h * 8; }
 // Overwrites out like launch_tx_species; ``scratch`` holds at least one job.  ``scratch_zero``:
 // the scratch is as an earlier call left it (otherwise it is cleared whole first).
-Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, const GridPlanDev& gp,
+Status launch_tx_gridding(const TxGrid& g, const SpeciesSet& sp, const GridPlanDev& gp,
                           const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,
                           const float2* tw_h, void* scratch, size_t scratch_bytes, bool scratch_zero, float2* out,
                           cudaStream_t st, int* launches);

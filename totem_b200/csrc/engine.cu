@@ -334,14 +334,15 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
   const RowsHost host_i = split_rows(a->proj_coff_mat_i, n_rows_i, nc_i, has_abs_i ? a->absorp_n_i : nullptr, beg_i);
   cim_len = a->cim_len;
   n_corr = n_corr_i = 0;
+  RowsHost host_cn, host_ci;
   if (cim_len > 0) {
     if (!a->corr_info_matrix) return Status::Err(TOTEM_ERR_INVALID_ARG, "corr_info_matrix is NULL");
     TOTEM_TRY(offsets(a->series_n_corr, slices, beg_cn, n_corr, "series_n_corr"));
     TOTEM_TRY(offsets(a->series_n_i_corr, slices, beg_ci, n_corr_i, "series_n_i_corr"));
     if ((n_corr > 0 && !a->ele_n_corr) || (n_corr_i > 0 && !a->ele_n_i_corr))
       return Status::Err(TOTEM_ERR_INVALID_ARG, "correction rows are NULL");
-    TOTEM_TRY(rows_cn.put(split_rows(a->ele_n_corr, n_corr, 5, nullptr, beg_cn), st));
-    TOTEM_TRY(rows_ci.put(split_rows(a->ele_n_i_corr, n_corr_i, 8, nullptr, beg_ci), st));
+    host_cn = split_rows(a->ele_n_corr, n_corr, 5, nullptr, beg_cn);
+    host_ci = split_rows(a->ele_n_i_corr, n_corr_i, 8, nullptr, beg_ci);
     const size_t plane = (size_t)p_h * p_w;
     std::vector<float> c(plane * cim_len);
     for (size_t i = 0; i < c.size(); ++i) c[i] = (float)a->corr_info_matrix[i];
@@ -357,16 +358,23 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
         separable = false;
         break;
       }
-  // neutral / ionic rows: by species on separable grids (k_tx_species), row by row otherwise
+  // neutral, ionic and correction rows: by species on separable grids (k_tx_species or
+  // gridding), row by row otherwise
   grid_ok = false;
   if (separable) {
     const totem::SpeciesHost spn = group_species(host_n, slices), spi = group_species(host_i, slices);
+    const totem::SpeciesHost spcn = group_species(host_cn, slices), spci = group_species(host_ci, slices);
     TOTEM_TRY(species_n.put(spn, st));
     TOTEM_TRY(species_i.put(spi, st));
-    TOTEM_TRY(plan_gridding(a, spn, spi));
+    TOTEM_TRY(species_cn.put(spcn, st));
+    TOTEM_TRY(species_ci.put(spci, st));
+    const totem::SpeciesHost* const kinds[4] = {&spn, &spi, &spcn, &spci};
+    TOTEM_TRY(plan_gridding(a, kinds));
   } else {
     TOTEM_TRY(rows_n.put(host_n, st));
     TOTEM_TRY(rows_i.put(host_i, st));
+    TOTEM_TRY(rows_cn.put(host_cn, st));
+    TOTEM_TRY(rows_ci.put(host_ci, st));
   }
   std::vector<float> s2f(plane);
   for (size_t i = 0; i < plane; ++i) s2f[i] = (float)a->s_2[i];
@@ -451,8 +459,11 @@ Status totem_session::build_transmission(int path, int* launches) {
   const auto vcn = rows_cn.view(cim_len > 0 && n_corr > 0, false, 3);
   const auto vci = rows_ci.view(cim_len > 0 && n_corr_i > 0, false, 6);
   if (separable) {
-    const auto sn = species_n.view(n_rows > 0, has_abs_n, ncoef_n);
-    const auto si = species_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
+    totem::SpeciesSet set;
+    set.k[0] = species_n.view(n_rows > 0, has_abs_n, ncoef_n);
+    set.k[1] = species_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
+    set.k[2] = species_cn.view(cim_len > 0 && n_corr > 0, false, 3);
+    set.k[3] = species_ci.view(cim_len > 0 && n_corr_i > 0, false, 6);
     const int mode = totem::tx_builder_mode();
     if (grid_ok && (mode == TOTEM_TX_GRIDDING || (mode == TOTEM_TX_AUTO && gridding_cheaper()))) {
       // jobs per batch from the budget for their planes (64 bytes per pixel); the row flags on top
@@ -471,7 +482,7 @@ Status totem_session::build_transmission(int path, int* launches) {
       const bool was_zero = grid_scratch_zero;
       grid_scratch_zero = false;  // until every batch has been enqueued
       ran_tx_builder = TOTEM_TX_GRIDDING;
-      TOTEM_TRY(totem::launch_tx_gridding(g, sn, si, gp, grid_job_beg_h, grid_jobs_h, tw_pw.as<float2>(),
+      TOTEM_TRY(totem::launch_tx_gridding(g, set, gp, grid_job_beg_h, grid_jobs_h, tw_pw.as<float2>(),
                                           tw_ph.as<float2>(), grid_scratch.p, bytes, was_zero, T.as<float2>(), stream,
                                           launches));
       grid_scratch_zero = true;  // left as the next build expects it (in stream order)
@@ -483,12 +494,7 @@ Status totem_session::build_transmission(int path, int* launches) {
       }
     } else {
       ran_tx_builder = TOTEM_TX_DIRECT;
-      TOTEM_TRY(totem::launch_tx_species(g, sn, si, T.as<float2>(), stream));
-      ++*launches;
-    }
-    if (vcn.beg || vci.beg) {  // Peng-extended correction rows: per-pixel maps, row by row
-      TOTEM_TRY(totem::launch_tx_structure(g, totem::AtomRowsDev{}, totem::AtomRowsDev{}, vcn, vci, T.as<float2>(),
-                                           stream, true));
+      TOTEM_TRY(totem::launch_tx_species(g, set, T.as<float2>(), stream));
       ++*launches;
     }
   } else {
@@ -520,9 +526,8 @@ Status totem_session::build_transmission(int path, int* launches) {
 // Uniform separable axes, kx(c) = kx0 + c dkx and ky(r) = ky0 + r dky (the reference's
 // meshgrid of (-P/2 : P/2-1) / (P dx), ToTEM_submit_v1.m:1534-1538), on power-of-two grids admit
 // the gridding builder.  Its job table holds one job per species segment of every slice
-// (neutral, then ionic), in slice order.
-Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::SpeciesHost& spn,
-                                    const totem::SpeciesHost& spi) {
+// (neutral, ionic, then the correction kinds), in slice order.
+Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::SpeciesHost* const (&kinds)[4]) {
   grid_ok = false;
   grid_job_beg_h.clear();
   grid_jobs_h.clear();
@@ -543,8 +548,8 @@ Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::Species
   grid_sy = a->ky[0] + dky * (p_h / 2);
   grid_job_beg_h.assign(slices + 1, 0);
   for (int s = 0; s < slices; ++s) {
-    for (int kind = 0; kind < 2; ++kind) {
-      const totem::SpeciesHost& sp = kind ? spi : spn;
+    for (int kind = 0; kind < 4; ++kind) {
+      const totem::SpeciesHost& sp = *kinds[kind];
       if ((int)sp.seg_beg.size() != slices + 1) continue;
       for (int q = sp.seg_beg[s]; q < sp.seg_beg[s + 1]; ++q) {
         grid_jobs_h.push_back(make_int4(kind, sp.seg[3 * q], sp.seg[3 * q + 1], sp.seg[3 * q + 2]));

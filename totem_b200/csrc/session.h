@@ -164,6 +164,7 @@ struct totem_session {
   totem::DevBuf probe, prop, mask_mid, mask_exit, tw_n, tw_pw, tw_ph, gfsf_d;
   totem::RowsDev rows_n, rows_i, rows_cn, rows_ci;
   totem::SpeciesRowsDev species_n, species_i;  // the neutral / ionic rows by species (separable grids)
+  totem::SpeciesRowsDev species_cn, species_ci;  // the correction rows by species (separable grids)
   // gridding builder (uniform separable axes): job table, deconvolution tables, work memory
   bool grid_ok = false;
   bool grid_scratch_zero = false;  // grid_scratch is as the last gridding build left it, for
@@ -224,7 +225,7 @@ struct totem_session {
       f(*b);
     for (totem::RowsDev* r : {&rows_n, &rows_i, &rows_cn, &rows_ci})
       for (totem::DevBuf* b : {&r->pos, &r->coef, &r->absorp, &r->beg}) f(*b);
-    for (totem::SpeciesRowsDev* r : {&species_n, &species_i})
+    for (totem::SpeciesRowsDev* r : {&species_n, &species_i, &species_cn, &species_ci})
       for (totem::DevBuf* b : {&r->pos, &r->coef, &r->absorp, &r->seg_beg, &r->seg}) f(*b);
   }
 
@@ -274,7 +275,7 @@ struct totem_session {
   static Status validate(const TotemStemArgs* a, bool stem);
   Status upload_args(const TotemStemArgs* a, bool stem);
   Status build_transmission(int path, int* launches);
-  Status plan_gridding(const TotemStemArgs* a, const totem::SpeciesHost& spn, const totem::SpeciesHost& spi);
+  Status plan_gridding(const TotemStemArgs* a, const totem::SpeciesHost* const (&kinds)[4]);
   bool gridding_cheaper() const;
   totem::DetectionEvents detection_events() const;
   // Per-event detector sums acc[event][w][A][depth] -> out_result (exit) and out_mid (layers),

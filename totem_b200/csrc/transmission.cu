@@ -65,6 +65,31 @@ __device__ __forceinline__ void row_form(int kind, int lobato, const float* cf, 
   fi = absorp != nullptr ? cf[0] * peng5(absorp, s2) : 0.f;
 }
 
+// Form factor of species ``sp`` of kind ``kind`` (SpeciesSet) at pixel ``pix`` (s^2 = s2):
+// kinds 0 / 1 as row_form; the Peng-extended correction kinds 2 / 3
+// (cuda_source_peng_and_corr.cu:587-779, GetPotential4AllSlice_multicore_lotabo_peng_corr.m:13-60)
+// amplitude * exp(-B s^2) * the correction plane(s) at the pixel (planes numbered from 1).
+__device__ __forceinline__ void species_form(int kind, const TxGrid& g, const SpeciesDev& d, int sp, float s2,
+                                             long pix, float& fr, float& fi) {
+  const float* cf = d.coef + (long)sp * d.ncoef;
+  if (kind <= 1) {
+    row_form(kind, g.lobato, cf, d.absorp != nullptr ? d.absorp + (long)sp * 10 : nullptr, s2, fr, fi);
+    return;
+  }
+  const long plane = (long)g.p_h * g.p_w;
+  float m = 0.f;
+  if (kind == 2) {
+    const int idx = (int)cf[2] - 1;
+    if (idx >= 0 && idx < g.cim_len) m = g.cim[idx * plane + pix];
+  } else {
+    const int i1 = (int)cf[3] - 1, i2 = (int)cf[5] - 1;
+    if (i1 >= 0 && i1 < g.cim_len) m = fmaf(cf[2], g.cim[i1 * plane + pix], m);
+    if (i2 >= 0 && i2 < g.cim_len) m = fmaf(cf[4], g.cim[i2 * plane + pix], m);
+  }
+  fr = cf[1] * m * __expf(-cf[0] * s2);
+  fi = 0.f;
+}
+
 // exp(-2 pi i t) for t given in FP64, reduced to [0, 1) before the FP32 evaluation.
 __device__ __forceinline__ float2 phase_of(double t) {
   const double fr = t - floor(t);
@@ -200,8 +225,7 @@ struct SpSmem {
   float4 ey[SP_CH][SP_T];
 };
 
-__global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesDev nr, SpeciesDev ir,
-                                                        float2* __restrict__ out) {
+__global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesSet spset, float2* __restrict__ out) {
   __shared__ SpSmem sm;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int slice = blockIdx.z;
@@ -211,8 +235,8 @@ __global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesDev nr, 
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
-  for (int kind = 0; kind < 2; ++kind) {
-    const SpeciesDev& d = kind ? ir : nr;
+  for (int kind = 0; kind < 4; ++kind) {
+    const SpeciesDev& d = spset.k[kind];
     if (d.seg_beg == nullptr) continue;
     const int s_end = d.seg_beg[slice + 1];
     for (int sidx = d.seg_beg[slice]; sidx < s_end; ++sidx) {
@@ -256,15 +280,14 @@ __global__ void __launch_bounds__(256, 2) k_tx_species(TxGrid g, SpeciesDev nr, 
           }
         }
       }
-      const float* cf = d.coef + (long)sp * d.ncoef;
-      const float* ab = d.absorp != nullptr ? d.absorp + (long)sp * 10 : nullptr;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int r = min(r_tile + ty + 16 * i, g.p_h - 1), c = min(c_tile + tx + 16 * j, g.p_w - 1);
+          const long pix = (long)r * g.p_w + c;
           float fr, fi;
-          row_form(kind, g.lobato, cf, ab, __ldg(g.s2 + (long)r * g.p_w + c), fr, fi);
+          species_form(kind, g, d, sp, __ldg(g.s2 + pix), pix, fr, fi);
           acc[i][j].x = fmaf(fr, S[i][j].x, fmaf(-fi, S[i][j].y, acc[i][j].x));
           acc[i][j].y = fmaf(fr, S[i][j].y, fmaf(fi, S[i][j].x, acc[i][j].y));
         }
@@ -313,12 +336,11 @@ constexpr int GR_W = 2 * GR_MSP;
 constexpr float GR_FIX = 4294967296.f;         // 2^32
 constexpr float GR_UNFIX = 1.f / 4294967296.f;
 
-__global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, int p_w, const double* __restrict__ pos_n,
-                                                     const double* __restrict__ pos_i, int job0,
+__global__ void __launch_bounds__(256) k_grid_spread(GridPlanDev gp, int p_h, int p_w, SpeciesSet spset, int job0,
                                                      unsigned long long* __restrict__ grid,
                                                      unsigned* __restrict__ row_used) {
   const int4 jb = gp.jobs[job0 + blockIdx.y];  // kind, species, first atom, end atom
-  const double* pos = jb.x ? pos_i : pos_n;
+  const double* pos = spset.k[jb.x & 3].pos;
   const long plane = (long)p_h * p_w;
   unsigned long long* base = grid + (long)blockIdx.y * 8 * plane;  // 4 planes of (re, im) pairs
   const int total = (jb.w - jb.z) * GR_W;
@@ -453,7 +475,7 @@ __global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCf
 // half-bin combination and deconvolution give S, then f_species(s^2) S is summed; PARAMETER *
 // APERTURE as in k_tx_species.  A slice whose first jobs ran in an earlier batch adds to what
 // that batch wrote.
-__global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, SpeciesDev ir, GridPlanDev gp,
+__global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesSet spset, GridPlanDev gp,
                                                       const float2* __restrict__ grid, int s_lo, int j_lo, int j_hi,
                                                       float2* __restrict__ out) {
   const long plane = (long)g.p_h * g.p_w;
@@ -472,10 +494,8 @@ __global__ void __launch_bounds__(256) k_grid_combine(TxGrid g, SpeciesDev nr, S
       const int4 jb = gp.jobs[jj];
       const float2* F = grid + (long)(jj - j_lo) * 4 * pstride + (long)qr * pitch + c;
       const float2 S = cadd(cmul(y0, F[0]), cmul(y1, F[2 * pstride]));
-      const SpeciesDev& d = jb.x ? ir : nr;
       float fr, fi;
-      row_form(jb.x, g.lobato, d.coef + (long)jb.y * d.ncoef, d.absorp != nullptr ? d.absorp + (long)jb.y * 10 : nullptr,
-               s2, fr, fi);
+      species_form(jb.x & 3, g, spset.k[jb.x & 3], jb.y, s2, i, fr, fi);
       acc.x = fmaf(fr, S.x, fmaf(-fi, S.y, acc.x));
       acc.y = fmaf(fr, S.y, fmaf(fi, S.x, acc.y));
     }
@@ -613,12 +633,11 @@ Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const At
   return cuda_status(cudaGetLastError(), "k_tx_structure");
 }
 
-Status launch_tx_species(const TxGrid& g, const SpeciesDev& neutral, const SpeciesDev& ion, float2* out,
-                         cudaStream_t st) {
+Status launch_tx_species(const TxGrid& g, const SpeciesSet& sp, float2* out, cudaStream_t st) {
   if (g.slices == 0) return Status::Ok();
   if (!g.separable) return Status::Err(TOTEM_ERR_UNSUPPORTED, "species builder needs separable reciprocal grids");
   dim3 grid((g.p_w + SP_T - 1) / SP_T, (g.p_h + SP_T - 1) / SP_T, g.slices);
-  k_tx_species<<<grid, 256, 0, st>>>(g, neutral, ion, out);
+  k_tx_species<<<grid, 256, 0, st>>>(g, sp, out);
   return cuda_status(cudaGetLastError(), "k_tx_species");
 }
 
@@ -657,7 +676,7 @@ std::vector<GridBatch> grid_batches(const std::vector<int>& job_beg, int jobs_pe
   return out;
 }
 
-Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDev& ir, const GridPlanDev& gp,
+Status launch_tx_gridding(const TxGrid& g, const SpeciesSet& sp, const GridPlanDev& gp,
                           const std::vector<int>& job_beg, const std::vector<int4>& jobs, const float2* tw_w,
                           const float2* tw_h, void* scratch, size_t scratch_bytes, bool scratch_zero, float2* out,
                           cudaStream_t st, int* launches) {
@@ -685,7 +704,7 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
       int most = 0;
       for (int j = b.j_lo; j < b.j_hi; ++j) most = std::max(most, jobs[j].w - jobs[j].z);
       const unsigned bx = (unsigned)std::min<long>(((long)most * GR_W + 255) / 256 + 1, 4096);
-      k_grid_spread<<<dim3(bx, nj), 256, 0, st>>>(gp, g.p_h, g.p_w, nr.pos, ir.pos, b.j_lo,
+      k_grid_spread<<<dim3(bx, nj), 256, 0, st>>>(gp, g.p_h, g.p_w, sp, b.j_lo,
                                                   static_cast<unsigned long long*>(scratch), used);
       TOTEM_TRY(cuda_status(cudaGetLastError(), "k_grid_spread"));
       const long pairs = (long)nj * 2 * g.p_h, planes = (long)nj * 2;  // (job, ey) after the row pass
@@ -713,7 +732,7 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesDev& nr, const SpeciesDe
     const unsigned cx = (unsigned)std::min<long>((plane + 255) / 256, 2048);
     for (int s0 = b.s_lo; s0 < b.s_hi; s0 += 65535) {
       const int ns = std::min(b.s_hi - s0, 65535);
-      k_grid_combine<<<dim3(cx, ns), 256, 0, st>>>(g, nr, ir, gp, static_cast<const float2*>(scratch), s0, b.j_lo,
+      k_grid_combine<<<dim3(cx, ns), 256, 0, st>>>(g, sp, gp, static_cast<const float2*>(scratch), s0, b.j_lo,
                                                    b.j_hi, out);
       TOTEM_TRY(cuda_status(cudaGetLastError(), "k_grid_combine"));
       ++*launches;

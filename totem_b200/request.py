@@ -188,6 +188,24 @@ def build_srtio3_stem(cells=(8, 8, 50), n: int = 512, sampling: float = 0.0625, 
                          native_slicing=native_slicing)
 
 
+def build_stem_on_structure(st: specimen.Structure, n: int = 512, sampling: float = 0.0625, step: int = 8,
+                            raster=(64, 64), p: Optional[int] = None, flag: str = PENG, kv: float = 300.0,
+                            semi_angle: float = 25.0, c3_um: float = -5.0, defocus_nm: float = 0.0,
+                            detectors=((60.0, 200.0), (0.0, 10.0)), mid_layer=(),
+                            native_slicing: bool = False, engine_optics: bool = False) -> StemRequest:
+    """The STEM-ADF probe, detectors and scan of ``build_srtio3_stem`` on any specimen, centred
+    on a potential grid of ``p`` (default: the scan plus one window, rounded up to a power of two)."""
+    need = n + (max(raster) - 1) * step
+    if p is None:
+        p = 1 << (need - 1).bit_length()
+    begin = ((p - (n + (raster[0] - 1) * step)) // 2, (p - (n + (raster[1] - 1) * step)) // 2)
+    st = specimen.center_in_field(st, p * sampling, p * sampling)
+    spec = optics.ProbeSpec(kv=kv, semi_angle_mrad=semi_angle,
+                            aberrations=optics.Aberrations(focus=defocus_nm, Cs=c3_um * 1e3))
+    return _stem_request(st, flag, kv, sampling, n, p, step, raster, begin, detectors, spec, mid_layer=mid_layer,
+                         native_slicing=native_slicing, engine_optics=engine_optics)
+
+
 def build_stem_from_table(atoms, eachthick: float, slicethick, n: int = 128, p: int = 256, sampling: float = 0.15,
                           step: int = 16, raster=(3, 3), flag: str = PENG, kv: float = 300.0,
                           semi_angle: float = 25.0, c3_um: float = -5.0, defocus_nm: float = 0.0,

@@ -19,7 +19,7 @@ from dataclasses import replace
 
 import numpy as np
 
-from . import capi, request
+from . import capi, request, specimen
 
 STEP = 8
 SAMPLING = 0.0625  # Angstrom per pixel
@@ -30,11 +30,18 @@ def _grid(n: int, rmax: int) -> int:
     return 1 << (need - 1).bit_length()
 
 
-def _base(n: int, flag: str, rmax: int, smax: int):
+def _base(n: int, flag: str, rmax: int, smax: int, what: str = "srtio3"):
+    """A supercell filling the potential grid of an n^2 window and an rmax^2 scan, ``smax`` slices
+    thick: SrTiO3 [001] (2 slices per 3.905 Angstrom cell) or Si [001] (4 per 5.431 Angstrom)."""
     p = _grid(n, rmax)
+    if what == "si":
+        cells = max(1, int(p * SAMPLING // 5.431))
+        st = specimen.si_001(cells, cells, (smax + 3) // 4)
+        return request.build_stem_on_structure(st, n=n, sampling=SAMPLING, step=STEP, raster=(rmax, rmax), p=p,
+                                               flag=flag, native_slicing=True, engine_optics=True)
     cells = max(1, int(p * SAMPLING // 3.905))
     return request.build_srtio3_stem(cells=(cells, cells, (smax + 1) // 2), n=n, sampling=SAMPLING, step=STEP,
-                                     raster=(rmax, rmax), p=p, flag=flag, native_slicing=True)
+                                     raster=(rmax, rmax), p=p, flag=flag, native_slicing=True, engine_optics=True)
 
 
 def derive(base, rows: int, cols: int, slices: int, mid_layer=()):
@@ -53,9 +60,10 @@ def derive(base, rows: int, cols: int, slices: int, mid_layer=()):
 
 
 def make_workload(count: int = 64, seed: int = 0, sizes=(256, 512), max_probes: int = 1024,
-                  slices=(20, 100)):
+                  slices=(20, 100), specimens=("srtio3",)):
     """``count`` seeded requests: window from ``sizes``, probes log-uniform in [1, max_probes],
-    slices uniform in ``slices``, Peng / Lobato half and half, a mid-layer detector on a third."""
+    slices uniform in ``slices``, Peng / Lobato half and half, a mid-layer detector on a third,
+    the supercell drawn from ``specimens`` ("srtio3", "si") when there is more than one."""
     rng = np.random.default_rng(seed)
     rmax = int(math.ceil(math.sqrt(max_probes)))
     bases = {}
@@ -63,14 +71,15 @@ def make_workload(count: int = 64, seed: int = 0, sizes=(256, 512), max_probes: 
     for _ in range(count):
         n = int(rng.choice(sizes))
         flag = "p" if rng.random() < 0.5 else "l"
-        if (n, flag) not in bases:
-            bases[(n, flag)] = _base(n, flag, rmax, slices[1])
+        what = str(rng.choice(specimens)) if len(specimens) > 1 else specimens[0]
+        if (n, flag, what) not in bases:
+            bases[(n, flag, what)] = _base(n, flag, rmax, slices[1], what)
         probes = int(round(math.exp(rng.uniform(0.0, math.log(max_probes)))))
         rows = min(rmax, int(math.ceil(math.sqrt(probes))))
         cols = min(rmax, max(1, int(math.ceil(probes / rows))))
         s = int(rng.integers(slices[0], slices[1] + 1))
         mid = (s // 2,) if rng.random() < 1 / 3 else ()
-        reqs.append(derive(bases[(n, flag)], rows, cols, s, mid))
+        reqs.append(derive(bases[(n, flag, what)], rows, cols, s, mid))
     return reqs
 
 
@@ -141,18 +150,31 @@ def main(argv=None):
     ap.add_argument("--prep-threads", type=int, default=0, help="server preparation threads (0 = its default)")
     ap.add_argument("--compare", action="store_true", help="also serve one request at a time")
     ap.add_argument("--burst-only", action="store_true", help="skip the Poisson-arrival runs")
+    ap.add_argument("--specimens", nargs="+", default=["srtio3"], choices=["srtio3", "si"])
+    ap.add_argument("--capacity-sample", type=int, default=0,
+                    help="measure the burst capacity on the first K requests only (0 = all of them)")
+    ap.add_argument("--check-alone", type=int, default=0,
+                    help="compare K seeded requests of the Poisson run with the same request alone")
+    ap.add_argument("--mixed-windows", action="store_true", help="one persistent launch for 256^2..1024^2 windows")
     ns = ap.parse_args(argv)
     policy = capi.SCHED_SHORTEST if ns.policy == "shortest" else capi.SCHED_FIFO
-    reqs = make_workload(ns.requests, ns.seed, tuple(ns.sizes), ns.max_probes, tuple(ns.slices))
+    t0 = time.perf_counter()
+    reqs = make_workload(ns.requests, ns.seed, tuple(ns.sizes), ns.max_probes, tuple(ns.slices), tuple(ns.specimens))
+    print(json.dumps({"workload_built_s": time.perf_counter() - t0, "requests": len(reqs),
+                      "probe_slices": int(sum(r.probe_slices for r in reqs))}), flush=True)
     kw = {"wave_bytes": ns.wave_mib << 20} if ns.wave_mib else {}
+    if ns.mixed_windows:
+        kw["mixed_windows"] = True
     if ns.chunk_mib:
         kw["chunk_bytes"] = ns.chunk_mib << 20
     if ns.prep_threads:
         kw["prep_threads"] = ns.prep_threads
     # warm-up (kernels, pools) on a few requests, then the burst capacity
     serve(reqs[:4], np.zeros(4), policy, **kw)
-    res_b, lat_b, mk_b = serve(reqs, np.zeros(len(reqs)), policy, **kw)
-    out = [dict(summary("burst", reqs, lat_b, mk_b), phases_mean=serve.last_phases, server=serve.last_stats)]
+    cap = reqs[:ns.capacity_sample] if ns.capacity_sample else reqs
+    res_b, lat_b, mk_b = serve(cap, np.zeros(len(cap)), policy, **kw)
+    out = [dict(summary("burst" if cap is reqs else f"burst (first {len(cap)})", cap, lat_b, mk_b),
+                phases_mean=serve.last_phases, server=serve.last_stats)]
     if ns.compare:
         _, lat_sb, mk_sb = serve_one_at_a_time(reqs, np.zeros(len(reqs)))
         out.append(summary("one-at-a-time burst", reqs, lat_sb, mk_sb))
@@ -160,11 +182,23 @@ def main(argv=None):
         for o in out:
             print(json.dumps(o), flush=True)
         return out
-    rate = ns.rate or ns.load * len(reqs) / mk_b
+    # offered load: a fraction of the burst capacity in probe*slices/s, in requests of this mix
+    capacity = sum(r.probe_slices for r in cap) / mk_b
+    rate = ns.rate or ns.load * capacity / np.mean([r.probe_slices for r in reqs])
     arr = poisson_arrivals(len(reqs), rate, ns.seed)
     res_p, lat_p, mk_p = serve(reqs, arr, policy, **kw)
     out.append(dict(summary("poisson", reqs, lat_p, mk_p), rate_hz=rate, phases_mean=serve.last_phases,
                     server=serve.last_stats))
+    sizes = sorted({r.height for r in reqs})
+    out[-1]["by_window"] = {str(n): {"requests": int(sum(r.height == n for r in reqs)),
+                                     "p50_ms": float(np.percentile([l for r, l in zip(reqs, lat_p) if r.height == n], 50)),
+                                     "p99_ms": float(np.percentile([l for r, l in zip(reqs, lat_p) if r.height == n], 99))}
+                            for n in sizes}
+    if ns.check_alone:
+        rng = np.random.default_rng(ns.seed + 2)
+        idx = sorted(rng.choice(len(reqs), size=min(ns.check_alone, len(reqs)), replace=False).tolist())
+        same = [bool(np.array_equal(res_p[i][0], capi.stem_run(reqs[i])[0])) for i in idx]
+        out[-1]["alone_vs_mix"] = {"checked": idx, "bit_identical": same}
     if ns.compare:
         res_s, lat_s, mk_s = serve_one_at_a_time(reqs, arr)
         out.append(dict(summary("one-at-a-time", reqs, lat_s, mk_s), rate_hz=rate))

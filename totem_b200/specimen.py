@@ -83,16 +83,19 @@ class Structure:
 
 
 def _tile(basis, cell, reps):
-    """Replicate a fractional basis [(Z, fx, fy, fz)] over ``reps`` cells of size ``cell``."""
+    """Replicate a fractional basis [(Z, fx, fy, fz)] over ``reps`` cells of size ``cell``: rows
+    ordered by cell z, then y, then x, then basis atom, with coordinates (i + fx) * ax etc."""
     nx, ny, nz = reps
     ax, ay, az = cell
-    out = []
-    for k in range(nz):
-        for j in range(ny):
-            for i in range(nx):
-                for zz, fx, fy, fz in basis:
-                    out.append((zz, (i + fx) * ax, (j + fy) * ay, (k + fz) * az))
-    return np.array(out, dtype=np.float64)
+    b = np.asarray(basis, dtype=np.float64)
+    k, j, i = np.meshgrid(np.arange(nz, dtype=np.float64), np.arange(ny, dtype=np.float64),
+                          np.arange(nx, dtype=np.float64), indexing="ij")
+    out = np.empty((nz, ny, nx, len(b), 4))
+    out[..., 0] = b[:, 0]
+    out[..., 1] = (i[..., None] + b[:, 1]) * ax
+    out[..., 2] = (j[..., None] + b[:, 2]) * ay
+    out[..., 3] = (k[..., None] + b[:, 3]) * az
+    return out.reshape(-1, 4)
 
 
 def _table(zxyz, dw=None, occ=1.0, z_shift=0.0):
@@ -180,6 +183,12 @@ def center_in_field(st: Structure, field_x: float, field_y: float) -> Structure:
 # Parameter rows (getpotentialpara_lotabo_peng.m)
 # ----------------------------------------------------------------------------------------------
 
+def _per_species(keys: np.ndarray, rowfn) -> np.ndarray:
+    """rowfn(key) for every row of ``keys`` (Z, or Z and valence), evaluated once per distinct key."""
+    uniq, inv = np.unique(keys, axis=0, return_inverse=True)
+    return np.array([rowfn(u) for u in uniq])[inv.reshape(-1)]
+
+
 def potential_params(x: np.ndarray, flag: str):
     """Split atoms into the 16-column "nuclear" table and the 28-column "partly ionic" table.
 
@@ -196,7 +205,7 @@ def potential_params(x: np.ndarray, flag: str):
         t[:, 1:4] = neutral[:, 1:4]
         t[:, 4] = neutral[:, 6]
         t[:, 5] = neutral[:, 7] * (1 - neutral[:, 5])
-        t[:, 6:16] = _interleave(np.array([element_params(z, flag) for z in neutral[:, 0]]))
+        t[:, 6:16] = _per_species(neutral[:, 0], lambda z: _interleave(element_params(int(z), flag))[0])
         nuc.append(t)
     full = x[x[:, 5] == 1]
     if len(full):
@@ -205,7 +214,7 @@ def potential_params(x: np.ndarray, flag: str):
         t[:, 1:4] = full[:, 1:4]
         t[:, 4] = full[:, 6]
         t[:, 5] = full[:, 7] * full[:, 5]
-        t[:, 6:16] = _interleave(np.array([ion_params(z, v) for z, v in full[:, [0, 4]]]))
+        t[:, 6:16] = _per_species(full[:, [0, 4]], lambda zv: _interleave(ion_params(int(zv[0]), int(zv[1])))[0])
         nuc.append(t)
     all_nuclear = np.concatenate(nuc) if nuc else np.zeros((0, 16))
     part = x[(x[:, 5] > 0) & (x[:, 5] < 1)]
@@ -216,9 +225,9 @@ def potential_params(x: np.ndarray, flag: str):
         t[:, 4] = part[:, 6]
         t[:, 5] = part[:, 7]
         t[:, 6] = part[:, 5]
-        t[:, 7:17] = _interleave(np.array([ion_params(z, v) for z, v in part[:, [0, 4]]]))
+        t[:, 7:17] = _per_species(part[:, [0, 4]], lambda zv: _interleave(ion_params(int(zv[0]), int(zv[1])))[0])
         t[:, 17] = 1 - part[:, 5]
-        t[:, 18:28] = _interleave(np.array([element_params(z, flag) for z in part[:, 0]]))
+        t[:, 18:28] = _per_species(part[:, 0], lambda z: _interleave(element_params(int(z), flag))[0])
         all_nuc_ion = t
     else:
         all_nuc_ion = np.zeros((0, 28))
