@@ -7,9 +7,10 @@ BF 0-10 mrad detectors.  Synthetic (seeded) structure; no dataset.
 
 One "step" is one complete STEM request on the device: transmission build (potential, FFT,
 exp) + slice loop for all 4096 probes + detector reduction, inputs already resident in HBM.
-``value`` = probe*slices per second over all ranks (weak scaling: every rank runs its own
-request).  ``e2e`` = the same metric through ``totem_stem_run`` with host buffers (upload,
-run, download every step).
+``value`` = probe*slices per second over all ranks: with ``--scaling weak`` (default) every rank
+runs its own request; with ``--scaling strong`` the request's scan rows are split over the ranks
+(the sharded path of ``totem_b200.shard``).  ``e2e`` = the same metric through ``totem_stem_run``
+with host buffers (upload, run, download every step).
 
 ``--impl reference`` times the FP64 CPU oracle (the NumPy restatement of the reference's CPU
 path; MATLAB is not available) on a bounded sample of the same workload with all host cores.
@@ -271,7 +272,8 @@ def workload_config(ns, req):
             "probes": req.depth, "slices": req.slices, "window": req.height, "potential_grid": req.p_height,
             "detectors": req.aper_num, "path": ns.path, "l2": "inputs larger than L2 (transmission stack "
             f"{req.slices * req.p_height * req.p_width * 8 / 2**20:.0f} MiB)",
-            "parallelism": f"probe shards, {ns.gpus} GPU(s), no collective in the data path"}
+            "parallelism": (f"scan rows split over {ns.gpus} GPUs" if ns.scaling == "strong" and ns.gpus > 1 else
+                            f"one request per GPU, {ns.gpus} GPU(s)") + ", no collective in the data path"}
 
 
 def main():
@@ -289,6 +291,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-comparators", action="store_true", help="skip the plain cuFFT and serving legs")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="weak: every rank runs the whole request; strong: the request's scan rows are split "
+                         "over the ranks (shard.band_request), each rank building its own transmission")
     ap.add_argument("--no-band-skip", action="store_true",
                     help="compute the wave columns the propagator zeroes too (totem_set_band_skip(0))")
     ns = ap.parse_args()
@@ -318,7 +323,15 @@ def main():
     # (the legacy default stream has handle 0, which the C ABI reads as "make your own stream")
     stream = torch.cuda.Stream()
     sess = capi.Session(device=local, stream=stream.cuda_stream)
-    sess.upload(req)
+    strong = ns.scaling == "strong" and ws > 1
+    if strong:
+        # the product's sharded path: contiguous bands of scan rows, one per rank, no collective
+        # in the data path (the A x depth detector images are gathered once, after the timing)
+        from totem_b200 import shard
+        r0, r1 = shard.row_bands(req.hight_red, ws)[rank]
+        sess.upload(shard.band_request(req, r0, r1))
+    else:
+        sess.upload(req)
 
     def step():
         sess.run(path=path, batch=ns.batch, col_variant=ns.col_variant)
@@ -347,7 +360,8 @@ def main():
         ms_total = float(t.item())
     ms_step = ms_total / ns.steps
     units = req.probe_slices
-    value = ws * units * ns.steps / (ms_total / 1000.0)
+    # weak: every rank did the whole request; strong: the ranks did one request together
+    value = (1 if strong else ws) * units * ns.steps / (ms_total / 1000.0)
 
     # per-kernel device times (events around every pass) for the roofline
     sess.run(path=path, batch=ns.batch, profile=True, col_variant=ns.col_variant)
@@ -356,7 +370,8 @@ def main():
     n2 = req.height * req.width
     roofline = None
     if path == capi.PATH_FUSED and tm.row_pass_launches:
-        alg_bytes = units * 3 * n2 * BYTES_PER_ELEM  # read psi, write psi, read T window
+        # this rank's units: the whole request (weak) or its band (strong)
+        alg_bytes = sess.req.probe_slices * 3 * n2 * BYTES_PER_ELEM  # read psi, write psi, read T window
         step_ms = tm.row_pass_ms + tm.col_pass_ms
         achieved = alg_bytes / (step_ms / 1000.0) / 1e9
         traffic = None
@@ -377,20 +392,22 @@ def main():
     # end to end through the C ABI with host buffers
     e2e = None
     if not ns.no_e2e:
-        capi.stem_run(req, path=path, batch=ns.batch)  # warm the default session
+        e2e_req = sess.req  # the whole request, or this rank's band of it
+        capi.stem_run(e2e_req, path=path, batch=ns.batch)  # warm the default session
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
         for _ in range(ns.steps):
-            capi.stem_run(req, path=path, batch=ns.batch)
+            capi.stem_run(e2e_req, path=path, batch=ns.batch)
         dt = time.perf_counter() - t0
         if dist:
             t = torch.tensor([dt], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt = float(t.item())
         h2d = tm.h2d_bytes
-        d2h = 8 * req.aper_num * req.depth * (1 + len(req.mid_layer))
-        e2e = {"value": ws * units * ns.steps / dt, "unit": "probe*slices/s", "h2d_bytes_per_step": int(h2d),
+        d2h = 8 * e2e_req.aper_num * e2e_req.depth * (1 + len(e2e_req.mid_layer))
+        e2e = {"value": (1 if strong else ws) * units * ns.steps / dt, "unit": "probe*slices/s",
+               "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "api": "totem_stem_run (host buffers)"}
 
     plain = serve = None
@@ -409,7 +426,8 @@ def main():
         line = {
             "metric": "STEM probe*slices/s", "value": value, "unit": "probe*slices/s", "n_gpus": ws,
             "steps": ns.steps, "warmup": ns.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (complex64; FP64 detector sums)",
+            "scaling": "strong" if strong else "weak", "vs_baseline": None,
+            "dtype": "f32 (complex64; FP64 detector sums)",
             "data": "synthetic (seeded SrTiO3 supercell, random-free probe)",
             "config": workload_config(ns, req), "batch": batch_used,
             "gpu_launches": launches * ns.steps, "clocks": clk.summary(), "roofline": roofline,
