@@ -217,6 +217,12 @@ TOTEM_API int totem_set_slice_graphs(int enable);
  * the propagator the caller passes; results equal those with every column computed.  1 = on
  * (default), 0 = off.  Process-wide; no counterpart in the reference. */
 TOTEM_API int totem_set_band_skip(int enable);
+/* Failure injection on the host, for tests of the error paths (no GPU fault is involved): after
+ * ``alloc_after`` further device allocations of the engine the next one fails once with
+ * TOTEM_ERR_OOM, as if the device were full (-1 = off); every ``prepare_every``-th request a server
+ * prepares fails in its preparation with TOTEM_ERR_STATE before it touches the device (0 = off).
+ * Process-wide; each call resets the counts.  No counterpart in the reference. */
+TOTEM_API int totem_inject_failures(long long alloc_after, int prepare_every);
 /* Launch shapes chosen by measurement (python -m totem_b200.tune writes the table): one JSON
  * object per line, {"device": "<cudaDeviceProp.name>", "n": <window edge>, "row_variant": r,
  * "col_variant": c, "batch_mib": b, ...}.  Runs whose TotemRunOptions leave row_variant,

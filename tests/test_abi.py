@@ -124,3 +124,9 @@ def test_noalloc_rejects_2048_windows_before_any_device_call(lib):
                                        fake, None)
     assert rc == capi.ERR_UNSUPPORTED
     assert "1024" in lib.totem_last_error().decode()
+
+
+def test_failure_injection_arguments(lib):
+    assert lib.totem_inject_failures(C.c_longlong(-2), 0) == capi.ERR_INVALID_ARG
+    assert lib.totem_inject_failures(C.c_longlong(-1), -1) == capi.ERR_INVALID_ARG
+    assert lib.totem_inject_failures(C.c_longlong(-1), 0) == capi.OK

@@ -172,6 +172,10 @@ bool band_skip_ok(int n, int band, int col_variant);
 TileSkip band_tiles(int n, int nblk);
 // Process-wide: skip the zero band where band_skip_ok (totem_set_band_skip; on by default).
 bool band_skip_enabled();
+// Host-side failure injection (totem_inject_failures): true when the next device allocation of
+// the engine, or the next server preparation, is to fail (each call counts one event).
+bool inject_alloc_failure();
+bool inject_prepare_failure();
 
 struct SliceLoopArgs {
   int n = 0;                       // window edge N (power of two)

@@ -43,6 +43,9 @@ thread_local std::string g_last_error;
 std::atomic<int> g_tx_mode{TOTEM_TX_AUTO};
 std::atomic<int> g_slice_graphs{1};
 std::atomic<int> g_band_skip{1};
+std::atomic<long long> g_fail_alloc_after{-1};  // allocations to let through before one fails; -1 off
+std::atomic<long long> g_fail_prepare_every{0};  // every k-th server preparation fails; 0 off
+std::atomic<long long> g_prepares{0};
 std::atomic<size_t> g_tx_scratch{0};
 
 int fail(const Status& s) {
@@ -232,6 +235,20 @@ void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
 int totem::tx_builder_mode() { return g_tx_mode.load(); }
 bool totem::slice_graphs_enabled() { return g_slice_graphs.load() != 0; }
 bool totem::band_skip_enabled() { return g_band_skip.load() != 0; }
+
+bool totem::inject_alloc_failure() {
+  long long left = g_fail_alloc_after.load();
+  while (left >= 0) {  // armed: count down, fail once at zero, then disarm
+    if (g_fail_alloc_after.compare_exchange_weak(left, left - 1)) return left == 0;
+  }
+  return false;
+}
+
+bool totem::inject_prepare_failure() {
+  const long long k = g_fail_prepare_every.load();
+  if (k <= 0) return false;
+  return (g_prepares.fetch_add(1) + 1) % k == 0;
+}
 size_t totem::tx_gridding_scratch() {
   const size_t b = g_tx_scratch.load();
   return b ? b : (1ull << 30);
@@ -1269,6 +1286,16 @@ int totem_tuned_config(int device, int n, int* row_variant, int* col_variant, lo
     }
     return Status::Ok();
   });
+}
+
+int totem_inject_failures(long long alloc_after, int prepare_every) {
+  if (alloc_after < -1 || prepare_every < 0)
+    return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "alloc_after must be >= -1 and prepare_every >= 0"));
+  g_fail_alloc_after.store(alloc_after);
+  g_fail_prepare_every.store(prepare_every);
+  g_prepares.store(0);
+  g_last_error.clear();
+  return TOTEM_OK;
 }
 
 int totem_set_band_skip(int enable) {

@@ -229,6 +229,8 @@ void totem_server::fail_all(const Status& s) {
 // prep: admission, upload, transmission build
 // ---------------------------------------------------------------------------------------------
 Status totem_server::prepare(Request* r) {
+  if (totem::inject_prepare_failure())
+    return Status::Err(TOTEM_ERR_STATE, "injected failure of the request's preparation");
   TOTEM_CUDA(cudaSetDevice(device));
   totem_session* s = nullptr;
   TOTEM_TRY(totem::create_session(device, nullptr, &s));

@@ -40,6 +40,7 @@ struct DevBuf {
   Status ensure(size_t bytes) {
     if (bytes == 0) bytes = 256;
     if (bytes <= cap) return Status::Ok();
+    if (inject_alloc_failure()) return Status::Err(TOTEM_ERR_OOM, "injected device allocation failure");
     release();
     if (pool) TOTEM_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool, st));
     else TOTEM_CUDA(cudaMalloc(&p, bytes));
