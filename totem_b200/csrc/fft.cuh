@@ -212,7 +212,14 @@ template <> struct Plan<128> { static constexpr int P = 16, S = 2; static conste
 template <> struct Plan<256> { static constexpr int P = 16, S = 2; static constexpr int R[3] = {16, 16, 1}; };
 template <> struct Plan<512> { static constexpr int P = 32, S = 2; static constexpr int R[3] = {32, 16, 1}; };
 template <> struct Plan<1024> { static constexpr int P = 32, S = 2; static constexpr int R[3] = {32, 32, 1}; };
+#ifndef TOTEM_PLAN2048_P16
+#define TOTEM_PLAN2048_P16 0
+#endif
+#if TOTEM_PLAN2048_P16  // 16 points per thread: half the registers, twice the threads per transform
+template <> struct Plan<2048> { static constexpr int P = 16, S = 3; static constexpr int R[3] = {16, 16, 8}; };
+#else
 template <> struct Plan<2048> { static constexpr int P = 32, S = 3; static constexpr int R[3] = {32, 8, 8}; };
+#endif
 template <> struct Plan<4096> { static constexpr int P = 32, S = 3; static constexpr int R[3] = {32, 16, 8}; };
 
 template <int N>
