@@ -131,10 +131,15 @@ bool tuned_entry(int device, int n, TuneEntry* out) {
     if (!path.empty() && read_tuning(path, &t).ok()) g_tune = std::move(t);
   }
   if (g_tune.empty()) return false;
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return false;
+  static std::map<int, std::string> names;  // device -> cudaDeviceProp::name (under g_tune_mu)
+  auto it = names.find(device);
+  if (it == names.end()) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return false;
+    it = names.emplace(device, std::string(prop.name)).first;
+  }
   for (const TuneEntry& e : g_tune)
-    if (e.n == n && e.device == prop.name) {
+    if (e.n == n && e.device == it->second) {
       *out = e;
       return true;
     }

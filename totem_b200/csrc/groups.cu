@@ -1,5 +1,8 @@
 // Continuous batching: row and column passes over groups of items of several requests, each
 // group at its own slice; per window size, or (mixed) over 256^2 .. 1024^2 windows at once.
+#include <map>
+#include <mutex>
+
 #include "slice_tiles.cuh"
 
 namespace totem {
@@ -176,13 +179,24 @@ Status launch_mixed_groups(bool row, const GroupDesc* groups, const int* work_be
   smem = std::max(smem, mixed_smem<1024>());
   const void* fn = row ? (const void*)k_row_mixed : (const void*)k_col_mixed;
   TOTEM_TRY(ensure_smem(fn, smem));
-  static int ctas = 0;  // resident CTAs of the whole GPU (both kernels: same shape and bounds)
+  // resident CTAs of the whole GPU (both kernels: same shape and bounds), per device
+  static std::mutex mu;
+  static std::map<int, int> ctas_of;
+  int dev = 0;
+  TOTEM_CUDA(cudaGetDevice(&dev));
+  int ctas = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = ctas_of.find(dev);
+    if (it != ctas_of.end()) ctas = it->second;
+  }
   if (ctas == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    TOTEM_CUDA(cudaGetDevice(&dev));
+    int sms = 0, per_sm = 0;
     TOTEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     TOTEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_row_mixed, kMixedThreads, smem));
     ctas = std::max(1, sms * std::max(per_sm, 1));
+    std::lock_guard<std::mutex> lk(mu);
+    ctas_of[dev] = ctas;
   }
   const unsigned grid = (unsigned)std::min<long>(units, ctas);
   if (row) k_row_mixed<<<grid, kMixedThreads, smem, st>>>(groups, work_begin, ngroups, tick, tw, queue);
