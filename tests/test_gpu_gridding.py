@@ -63,11 +63,15 @@ def test_gridding_ionic_absorptive_and_vacuum_slices(engine_lib):
     assert np.all(grid[0] == 1.0) and np.all(grid[3] == 1.0)  # V = 0 exactly in vacuum slices
 
 
-def test_correction_rows_both_builders(engine_lib):
+@pytest.mark.parametrize("per_element", [False, True])
+def test_correction_rows_both_builders(engine_lib, per_element):
     # Peng-extended correction rows (per-pixel planes) summed by species in either builder: the
     # structure factor of each group of identical correction rows times its amplitude, Debye-Waller
     # envelope and plane(s); and on a non-separable grid by the per-atom kernel
-    req = request.with_correction(request.build_small_stem(flag="p"))
+    # per_element: few distinct rows per slice, summed by species; otherwise nearly every row is
+    # distinct and the rows are added by the per-atom kernel
+    req = request.with_correction(request.build_small_stem(flag="p"), every=1 if per_element else 4,
+                                  per_element=per_element)
     ref = so.transmission(req)
     assert rel_l2(ref, so.transmission(replace(req, corr_info_matrix=None))) > 10 * TOL  # rows matter
     direct, grid = _both(req)

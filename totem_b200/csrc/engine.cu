@@ -388,9 +388,20 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
     const totem::SpeciesHost spcn = group_species(host_cn, slices), spci = group_species(host_ci, slices);
     TOTEM_TRY(species_n.put(spn, st));
     TOTEM_TRY(species_i.put(spi, st));
-    TOTEM_TRY(species_cn.put(spcn, st));
-    TOTEM_TRY(species_ci.put(spci, st));
-    const totem::SpeciesHost* const kinds[4] = {&spn, &spi, &spcn, &spci};
+    // Correction rows share a form factor when they share B, amplitude and plane, i.e. per element
+    // (CalAllEquilent20210305_peng_corr.m); rows that are nearly all distinct are cheaper per atom
+    const size_t corr_rows = (size_t)n_corr + n_corr_i, corr_species = (spcn.seg.size() + spci.seg.size()) / 3;
+    corr_by_species = corr_rows == 0 || corr_species * 4 <= corr_rows;
+    const totem::SpeciesHost none;
+    if (corr_by_species) {
+      TOTEM_TRY(species_cn.put(spcn, st));
+      TOTEM_TRY(species_ci.put(spci, st));
+    } else {
+      TOTEM_TRY(rows_cn.put(host_cn, st));
+      TOTEM_TRY(rows_ci.put(host_ci, st));
+    }
+    const totem::SpeciesHost* const kinds[4] = {&spn, &spi, corr_by_species ? &spcn : &none,
+                                                corr_by_species ? &spci : &none};
     TOTEM_TRY(plan_gridding(a, kinds));
   } else {
     TOTEM_TRY(rows_n.put(host_n, st));
@@ -484,8 +495,10 @@ Status totem_session::build_transmission(int path, int* launches) {
     totem::SpeciesSet set;
     set.k[0] = species_n.view(n_rows > 0, has_abs_n, ncoef_n);
     set.k[1] = species_i.view(n_rows_i > 0, has_abs_i, ncoef_i);
-    set.k[2] = species_cn.view(cim_len > 0 && n_corr > 0, false, 3);
-    set.k[3] = species_ci.view(cim_len > 0 && n_corr_i > 0, false, 6);
+    if (corr_by_species) {
+      set.k[2] = species_cn.view(cim_len > 0 && n_corr > 0, false, 3);
+      set.k[3] = species_ci.view(cim_len > 0 && n_corr_i > 0, false, 6);
+    }
     const int mode = totem::tx_builder_mode();
     if (grid_ok && (mode == TOTEM_TX_GRIDDING || (mode == TOTEM_TX_AUTO && gridding_cheaper()))) {
       // jobs per batch from the budget for their planes (64 bytes per pixel); the row flags on top
@@ -517,6 +530,11 @@ Status totem_session::build_transmission(int path, int* launches) {
     } else {
       ran_tx_builder = TOTEM_TX_DIRECT;
       TOTEM_TRY(totem::launch_tx_species(g, set, T.as<float2>(), stream));
+      ++*launches;
+    }
+    if (!corr_by_species && (vcn.beg || vci.beg)) {  // nearly distinct correction rows: per atom, added
+      TOTEM_TRY(totem::launch_tx_structure(g, totem::AtomRowsDev{}, totem::AtomRowsDev{}, vcn, vci, T.as<float2>(),
+                                           stream, true));
       ++*launches;
     }
   } else {

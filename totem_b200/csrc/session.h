@@ -166,6 +166,8 @@ struct totem_session {
   totem::RowsDev rows_n, rows_i, rows_cn, rows_ci;
   totem::SpeciesRowsDev species_n, species_i;  // the neutral / ionic rows by species (separable grids)
   totem::SpeciesRowsDev species_cn, species_ci;  // the correction rows by species (separable grids)
+  // correction rows by species (few distinct rows per slice), or by the per-atom kernel on top
+  bool corr_by_species = true;
   // gridding builder (uniform separable axes): job table, deconvolution tables, work memory
   bool grid_ok = false;
   bool grid_scratch_zero = false;  // grid_scratch is as the last gridding build left it, for

@@ -291,12 +291,19 @@ def with_ionic_oxygen(req: StemRequest, every: int = 3, ion_fraction: float = 0.
     return replace(req, ele_n=rows[keep], series_n=series_n, ele_n_i=ion_rows, series_n_i=series_i)
 
 
-def with_correction(req: StemRequest, seed: int = 2, every: int = 4) -> StemRequest:
+def with_correction(req: StemRequest, seed: int = 2, every: int = 4, per_element: bool = False) -> StemRequest:
     """Attach synthetic Peng-extended correction rows to a request (tests only): two correction
     planes (cim) on the potential grid, a neutral row (x, y, B, amplitude, plane) at every
     ``every``-th atom and an ionic row (x, y, B, amplitude, w1, plane1, w2, plane2) at every
-    ``2 every``-th, keeping the atoms' slices."""
+    ``2 every``-th, keeping the atoms' slices.  The values are drawn per row, or with
+    ``per_element`` once per distinct coefficient row (element), as ToTem's rows are."""
     rng = np.random.default_rng(seed)
+    if per_element:
+        elem = np.unique(req.ele_n[:, 3:13], axis=0, return_inverse=True)[1].reshape(-1)
+        ne = int(elem.max()) + 1 if len(elem) else 0
+        table_n = [[rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), 1 + e % 2] for e in range(ne)]
+        table_i = [[rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), rng.uniform(0, 1), 1, rng.uniform(0, 1), 2]
+                   for _ in range(ne)]
     cim = np.stack([np.exp(-req.s2 * rng.uniform(0.5, 3.0)) * rng.uniform(0.5, 1.5, size=req.s2.shape)
                     for _ in range(2)])
     beg = np.concatenate([[0], np.cumsum(req.series_n)]).astype(int)
@@ -305,11 +312,13 @@ def with_correction(req: StemRequest, seed: int = 2, every: int = 4) -> StemRequ
         for a in range(beg[k], beg[k + 1]):
             x, y = req.ele_n[a, 0], req.ele_n[a, 1]
             if a % every == 0:
-                n_rows.append([x, y, rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), 1 + a % 2])
+                n_rows.append([x, y] + (table_n[elem[a]] if per_element else
+                                        [rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), 1 + a % 2]))
                 n_cnt[k] += 1
             if a % (2 * every) == 1:
-                i_rows.append([x, y, rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), rng.uniform(0, 1), 1,
-                               rng.uniform(0, 1), 2])
+                i_rows.append([x, y] + (table_i[elem[a]] if per_element else
+                                        [rng.uniform(0.5, 5.0), rng.uniform(0.1, 1.0), rng.uniform(0, 1), 1,
+                                         rng.uniform(0, 1), 2]))
                 i_cnt[k] += 1
     return replace(req, corr_info_matrix=cim, series_n_corr=n_cnt, series_n_i_corr=i_cnt,
                    ele_n_corr=np.asarray(n_rows, dtype=float).reshape(-1, 5),

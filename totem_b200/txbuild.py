@@ -7,7 +7,7 @@ difference of the two transmission stacks (on the first ``--check-slices`` slice
     python -m totem_b200.txbuild --grids 1024 2048 4096 --slices 20
 
 ``--correction`` adds Peng-extended correction rows (a neutral row for every atom, an ionic row for
-every second, two correction planes) and ``--per-atom`` also times the per-atom kernel, which every
+every second, two correction planes, values per element as in ToTem) and ``--per-atom`` also times the per-atom kernel, which every
 kind of row takes when the reciprocal grid is not the separable meshgrid (forced here by a relative
 change of 1e-12 in every other row of kx).
 """
@@ -72,7 +72,7 @@ def main(argv=None):
     for p in ns.grids:
         req = grid_filling_request(p, ns.slices, ns.flag)
         if ns.correction:
-            req = request.with_correction(req, every=1)
+            req = request.with_correction(req, every=1, per_element=True)
         atoms = int(np.sum(req.series_n) + np.sum(req.series_n_i))
         corr_rows = 0 if req.series_n_corr is None else int(np.sum(req.series_n_corr) + np.sum(req.series_n_i_corr))
         d_ms, d_l = build_ms(req, capi.TX_DIRECT, ns.reps)
