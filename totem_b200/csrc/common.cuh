@@ -28,9 +28,6 @@ Status cuda_status(cudaError_t e, const char* what);
 Status cufft_status(cufftResult r, const char* what);
 // Raise a kernel's dynamic shared-memory limit once (cached per function pointer).
 Status ensure_smem(const void* func, size_t bytes);
-// CTAs of ``func`` resident on the whole current device at once (``block`` threads, ``smem`` bytes
-// of dynamic shared memory), cached; 0 if the query fails.
-int resident_ctas(const void* func, int block, size_t smem);
 // Set the calling thread's message returned by totem_last_error().
 void set_last_error(const std::string& msg);
 

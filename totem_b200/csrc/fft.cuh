@@ -434,16 +434,8 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
-// Fetch the 128-byte line holding ``p`` into L2 ahead of its use (no register is written).
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// The slice-loop passes fetch the wave tile of the CTA one resident wave ahead into L2 while they
-// transform their own (TOTEM_L2_PREFETCH = 1).
-#ifndef TOTEM_L2_PREFETCH
-#define TOTEM_L2_PREFETCH 0
-#endif
 
 // Launch shapes shared by the kernels that transform whole rows or whole columns.
 // Rows: G transforms of T threads per CTA (each transform inside one warp, or a named barrier

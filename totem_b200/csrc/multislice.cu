@@ -32,18 +32,12 @@ namespace {
 // The launch covers the tiles outside [skip.z0, skip.z0 + skip.nskip) only.
 template <int N, bool PREFETCH, int CTAS128, int GW>
 __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
-    k_col_pass(SliceLoopArgs a, int flags, TileSkip skip, int ahead) {
+    k_col_pass(SliceLoopArgs a, int flags, TileSkip skip) {
   constexpr int G = ColCfg<N, CTAS128, GW>::G;
   constexpr int nblk = N / G;
   const int active = nblk - skip.nskip;
   const int item = blockIdx.x / active, t = blockIdx.x - item * active;
   const int cb = t < skip.z0 ? t : t + skip.nskip;
-  if (TOTEM_L2_PREFETCH && ahead > 0 && blockIdx.x + ahead < gridDim.x) {
-    // the column tile of the CTA ``ahead`` launch positions on (one resident wave): its rows into L2
-    const int f = blockIdx.x + ahead, fi = f / active, ft = f - fi * active;
-    const float2* fb = a.psi + (long)fi * N * N + (ft < skip.z0 ? ft : ft + skip.nskip) * G;
-    for (int r = threadIdx.x; r < N; r += blockDim.x) prefetch_l2(fb + (long)r * N);
-  }
   const ColInputs in{a.prop, a.mask_mid, a.mask_exit, a.aper_num, a.part_mid, a.part_exit};
   col_tile<N, PREFETCH, G>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw);
 }
@@ -77,9 +71,8 @@ Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
   TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128, GW>, smem));
   const TileSkip skip = a.skip_band ? band_tiles(N, N / G) : TileSkip();
-  const int ahead = TOTEM_L2_PREFETCH ? resident_ctas((const void*)k_col_pass<N, PREFETCH, CTAS128, GW>, G * T, smem) : 0;
   k_col_pass<N, PREFETCH, CTAS128, GW>
-      <<<(unsigned)((long)a.items * (N / G - skip.nskip)), G * T, smem, st>>>(a, flags, skip, ahead);
+      <<<(unsigned)((long)a.items * (N / G - skip.nskip)), G * T, smem, st>>>(a, flags, skip);
   TOTEM_TRY(cuda_status(cudaGetLastError(), "k_col_pass"));
   if ((flags & 8) && skip.nskip) {
     // a kept spectrum is stored whole: on the skipped columns it is exactly zero (the propagator is)

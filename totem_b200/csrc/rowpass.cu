@@ -10,19 +10,8 @@ namespace {
 // of RowCfg; the row-pass variants 3, 4, 5).  SKIP: leave out the zero-band columns.
 template <int N, bool FIRST, bool TB16, int CTAS = 0, bool SKIP = false>
 __global__ void __launch_bounds__(RowCfg<N, CTAS>::G * RowCfg<N, CTAS>::T, RowCfg<N, CTAS>::MINB)
-    k_row_pass(SliceLoopArgs a, const void* __restrict__ tslice, float scale, int ahead) {
+    k_row_pass(SliceLoopArgs a, const void* __restrict__ tslice, float scale) {
   constexpr int G = RowCfg<N>::G;
-  if (TOTEM_L2_PREFETCH && !FIRST && ahead > 0 && blockIdx.x + ahead < gridDim.x) {
-    // the G rows of the CTA ``ahead`` launch positions on (one resident wave) into L2, 128-byte
-    // lines, the zero-band columns left out when they are skipped
-    constexpr int lines = N * (int)sizeof(float2) / 128, per_line = 128 / (int)sizeof(float2);
-    const float2* fb = a.psi + (long)(blockIdx.x + ahead) * G * N;
-    for (int l = threadIdx.x; l < G * lines; l += blockDim.x) {
-      const int r = l / lines, c = (l - r * lines) * per_line;
-      if (SKIP && c >= BandCols<N>::lo && c < BandCols<N>::hi) continue;
-      prefetch_l2(fb + (long)r * N + c);
-    }
-  }
   using TElem = std::conditional_t<TB16, __nv_bfloat162, float2>;
   const long grow0 = (long)blockIdx.x * G;  // G divides N: the CTA's rows belong to one item
   const int item = (int)(grow0 / N), row0 = (int)(grow0 % N);
@@ -42,8 +31,7 @@ Status row_pass_launch(const SliceLoopArgs& a, const void* tslice, cudaStream_t 
   TOTEM_TRY(ensure_smem((const void*)k_row_pass<N, FIRST, TB16, CTAS, SKIP>, smem));
   const long rows = (long)a.items * N;
   const float scale = FIRST ? 1.f : 1.f / ((float)N * (float)N);
-  const int ahead = TOTEM_L2_PREFETCH ? resident_ctas((const void*)k_row_pass<N, FIRST, TB16, CTAS, SKIP>, G * T, smem) : 0;
-  k_row_pass<N, FIRST, TB16, CTAS, SKIP><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale, ahead);
+  k_row_pass<N, FIRST, TB16, CTAS, SKIP><<<(unsigned)(rows / G), G * T, smem, st>>>(a, tslice, scale);
   return cuda_status(cudaGetLastError(), "k_row_pass");
 }
 

@@ -38,22 +38,6 @@ Status ensure_smem(const void* func, size_t bytes) {
   return Status::Ok();
 }
 
-int resident_ctas(const void* func, int block, size_t smem) {
-  static std::mutex mu;
-  static std::map<std::pair<const void*, int>, int> done;  // one entry per (kernel, device)
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-  const auto key = std::make_pair(func, dev);
-  std::lock_guard<std::mutex> lk(mu);
-  auto it = done.find(key);
-  if (it != done.end()) return it->second;
-  int sms = 0, per_sm = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, block, smem) != cudaSuccess)
-    return 0;
-  return done[key] = sms * per_sm;
-}
-
 namespace {
 
 __global__ void k_d2f2(const double* __restrict__ re, const double* __restrict__ im, float2* __restrict__ out,
