@@ -29,7 +29,8 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
                      "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", INCLUDE]
-CU_SOURCES = ["util.cu", "transmission.cu", "multislice.cu", "rowpass.cu", "groups.cu", "hrtem.cu", "optics.cu", "plain.cu", "engine.cu",
+CU_SOURCES = ["util.cu", "transmission.cu", "multislice.cu", "rowpass.cu", "groups.cu",
+              "windows_mr_a.cu", "windows_mr_b.cu", "windows_mr_c.cu", "windows_mr_d.cu", "hrtem.cu", "optics.cu", "plain.cu", "engine.cu",
               "noalloc.cu", "server.cu", "specimen.cpp"]
 SHIMS = {  # library name -> (param flag, transmission flag)
     "libwaveCudaPeng.so": (0, 0),

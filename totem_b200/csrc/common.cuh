@@ -178,7 +178,7 @@ bool inject_alloc_failure();
 bool inject_prepare_failure();
 
 struct SliceLoopArgs {
-  int n = 0;                       // window edge N (power of two)
+  int n = 0;                       // window edge N (fused_window_ok)
   int items = 0;                   // items in this batch
   int item0 = 0;                   // first global item (w-major: item = w * depth + pos)
   ScanGeom geo{};
@@ -246,6 +246,25 @@ Status launch_mixed_groups(bool row, const GroupDesc* groups, const int* work_be
 // ``skip``: column tiles left out of the launch, wholly inside the zero band of every group in it
 Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                          const float2* tw, TileSkip skip, cudaStream_t st);
+
+// Square windows the fused passes take: powers of two 64..2048, and the mixed-radix edges of
+// TOTEM_MR_WINDOWS in fft.cuh (2^a times 3, 5, 7, 9 or 25, 96..1600).
+bool fused_window_ok(int n);
+// The entry points of one mixed-radix window size (their default launch shapes), which the
+// power-of-two dispatchers above fall through to; nullptr when n is not such a size.
+struct WindowOps {
+  int n;
+  int col_tiles;         // column tiles (detector partial sums) per probe
+  int band_lo, band_hi;  // BandCols<n>
+  Status (*row_pass)(const SliceLoopArgs& a, const void* tslice, bool first, cudaStream_t st);
+  Status (*col_pass)(const SliceLoopArgs& a, int flags, cudaStream_t st);
+  Status (*row_groups)(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                       const float2* tw, cudaStream_t st);
+  Status (*col_groups)(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
+                       const float2* tw, TileSkip skip, cudaStream_t st);
+  std::vector<float2> (*twiddles)();
+};
+const WindowOps* radix_window_ops(int n);
 
 // HRTEM imaging from the exit-wave spectrum spec [N][N] (FFT order): the exit wave
 // IFFT2(spec)/N^2 (complex64), and the image sum_k w_k |IFFT2(spec .* tf_k)/N^2|^2 (float32).

@@ -658,10 +658,12 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   const std::vector<int>& event_of_slice = de.event_of_slice;
   const int n_events = de.n_events, exit_event = de.exit_event;
 
-  const bool fused = (path != TOTEM_PATH_PLAIN) && h == w && is_pow2(h) && h >= 64 && h <= 2048 && slices > 0;
+  const bool fused = (path != TOTEM_PATH_PLAIN) && h == w && totem::fused_window_ok(h) && slices > 0;
   if (path == TOTEM_PATH_FUSED_ONLY && !fused && slices > 0)
     return Status::Err(TOTEM_ERR_UNSUPPORTED,
-                       "TOTEM_PATH_FUSED_ONLY: the fused slice loop needs a square power-of-two window of 64..2048");
+                       "TOTEM_PATH_FUSED_ONLY: the fused slice loop needs a square window of 64..2048, a power of "
+                       "two or a mixed-radix edge (96, 160, 192, 288, 320, 384, 400, 448, 576, 640, 768, 800, "
+                       "1152, 1280, 1536, 1600)");
   ran_slice_path = fused ? TOTEM_PATH_FUSED : TOTEM_PATH_PLAIN;
   const size_t vol = (size_t)h * w;
   int B = batch;
@@ -1004,6 +1006,7 @@ Status totem_session::run(int what, const TotemRunOptions* opt) {
           batch = (int)std::max<long long>(1, e.batch_bytes / ((long long)h * w * (long long)sizeof(float2)));
       }
     }
+    if (h == w && totem::radix_window_ops(h)) rv = cv = 0;  // mixed-radix windows: default shapes only
     used_row_variant = rv ? rv : 1;
     used_col_variant = cv ? cv : 1;
     TOTEM_TRY(slice_loop(o.path, batch, cv, o.t_storage, &launches, &batch_used, rv));

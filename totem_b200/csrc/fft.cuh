@@ -11,7 +11,9 @@
 //   R   :  8x8   16x8    16x16    32x16    32x32    32x8x8     32x16x8
 // so N <= 1024 needs one shared-memory exchange per transform.  Radix-16 and radix-32
 // butterflies run in registers as 4x4 and 8x4 Cooley-Tukey splits whose internal twiddles are
-// compile-time constants.  Inter-stage twiddles W_N^e = exp(-2 pi i e / N) come from per-stage
+// compile-time constants.  Mixed-radix windows (96 .. 1600, TOTEM_PLAN below) add radices with
+// a factor 3, 5 or 7 (odd primes from the DFT definition folded over conjugate pairs, composites
+// such as 24 = 8 x 3 by the same Cooley-Tukey split); their T = N / P need not be a power of two.  Inter-stage twiddles W_N^e = exp(-2 pi i e / N) come from per-stage
 // tables (index (r-1)*Ns + k) computed on the host in FP64, rounded once to FP32 and staged in
 // shared memory; lanes with consecutive k read consecutive entries, so the reads are free of bank
 // conflicts.  Exchanges use XOR-swizzled addresses chosen so that every 64-bit store and load of
@@ -81,7 +83,8 @@ constexpr double ce_cos_frac(int e, int R) {
     default: return ce_poly_cos(2 * kPi - x);
   }
 }
-constexpr double ce_sin_frac(int e, int R) { return ce_cos_frac(e - R / 4, R); }
+// sin(2 pi e / R) = cos(2 pi (4 e - R) / (4 R)), exact in integers for every R
+constexpr double ce_sin_frac(int e, int R) { return ce_cos_frac(4 * (e % R) - R, 4 * R); }
 
 // x * W_R^e (forward: exp(-2 pi i e/R)); inverse uses the conjugate.  Trivial angles are exact.
 template <int E, int R, bool INV>
@@ -193,6 +196,49 @@ __device__ __forceinline__ void dft_split(float2* x) {
   }
 }
 
+// Odd prime R straight from the definition, folded over conjugate pairs: with
+// a_m = x_m + x_{R-m}, b_m = x_m - x_{R-m} (m = 1 .. (R-1)/2) and theta = 2 pi m k / R,
+//   X_k     = x_0 + sum_m a_m cos(theta) - i sum_m b_m sin(theta)
+//   X_{R-k} = x_0 + sum_m a_m cos(theta) + i sum_m b_m sin(theta)
+// (forward; the inverse swaps the two signs of i).  The cosines and sines are compile-time
+// constants of the series above.
+template <int R, bool INV>
+__device__ __forceinline__ void dft_odd_prime(float2* x) {
+  constexpr int H = (R - 1) / 2;
+  float2 a[H], b[H];
+#pragma unroll
+  for (int m = 1; m <= H; ++m) {
+    a[m - 1] = cadd(x[m], x[R - m]);
+    b[m - 1] = csub(x[m], x[R - m]);
+  }
+  float2 out[R];
+  float2 s = x[0];
+#pragma unroll
+  for (int m = 0; m < H; ++m) s = cadd(s, a[m]);
+  out[0] = s;
+  static_for<1, H + 1>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    float2 re = x[0], im = make_float2(0.f, 0.f);
+    static_for<1, H + 1>([&](auto mc) {
+      constexpr int m = decltype(mc)::value;
+      constexpr float c = (float)ce_cos_frac(m * k, R), sn = (float)ce_sin_frac(m * k, R);
+      re = __ffma2_rn(make_float2(c, c), a[m - 1], re);
+      im = __ffma2_rn(make_float2(sn, sn), b[m - 1], im);
+    });
+    out[k] = cadd_rot<INV, 1>(re, im);       // re - i im (forward)
+    out[R - k] = cadd_rot<INV, -1>(re, im);  // re + i im (forward)
+  });
+#pragma unroll
+  for (int k = 0; k < R; ++k) x[k] = out[k];
+}
+
+constexpr bool ce_pow2(int r) { return r > 0 && (r & (r - 1)) == 0; }
+constexpr int ce_odd_factor(int r) {  // smallest odd prime factor (r not a power of two)
+  for (int p = 3; p <= r; p += 2)
+    if (r % p == 0) return p;
+  return r;
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft_r(float2* x) {
   if constexpr (R == 2) dft2<INV>(x);
@@ -200,6 +246,9 @@ __device__ __forceinline__ void dft_r(float2* x) {
   else if constexpr (R == 8) dft8<INV>(x);
   else if constexpr (R == 16) dft_split<4, 4, INV>(x);
   else if constexpr (R == 32) dft_split<8, 4, INV>(x);
+  else if constexpr (!ce_pow2(R) && ce_odd_factor(R) == R) dft_odd_prime<R, INV>(x);
+  else if constexpr (!ce_pow2(R)) dft_split<R / ce_odd_factor(R), ce_odd_factor(R), INV>(x);  // e.g. 24 = 8 x 3
+  else static_assert(R <= 32, "radix");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -222,13 +271,47 @@ template <> struct Plan<2048> { static constexpr int P = 32, S = 3; static const
 #endif
 template <> struct Plan<4096> { static constexpr int P = 32, S = 3; static constexpr int R[3] = {32, 16, 8}; };
 
+// Windows of 2^a x 3, 5, 7, 9 or 25 (multiples of 16, the window sizes the reference's STEM
+// driver can pack): every radix divides P, so T = N / P need not be a power of two (transform
+// groups that do not fit a warp evenly synchronise the whole CTA, see group_sync).
+#define TOTEM_PLAN(NN, PP, SS, R0_, R1_, R2_)                        \
+  template <>                                                        \
+  struct Plan<NN> {                                                  \
+    static constexpr int P = PP, S = SS;                             \
+    static constexpr int R[3] = {R0_, R1_, R2_};                     \
+  };
+TOTEM_PLAN(96, 24, 2, 24, 4, 1)
+TOTEM_PLAN(160, 20, 3, 20, 4, 2)
+TOTEM_PLAN(192, 24, 2, 24, 8, 1)
+TOTEM_PLAN(288, 24, 2, 24, 12, 1)
+TOTEM_PLAN(320, 20, 3, 20, 4, 4)
+TOTEM_PLAN(384, 24, 3, 24, 4, 4)
+TOTEM_PLAN(400, 20, 2, 20, 20, 1)
+TOTEM_PLAN(448, 28, 3, 28, 4, 4)
+TOTEM_PLAN(576, 24, 2, 24, 24, 1)
+TOTEM_PLAN(640, 40, 3, 40, 8, 2)
+TOTEM_PLAN(768, 24, 3, 24, 8, 4)
+TOTEM_PLAN(800, 20, 3, 20, 20, 2)
+TOTEM_PLAN(1152, 24, 3, 24, 24, 2)
+TOTEM_PLAN(1280, 40, 3, 40, 8, 4)
+TOTEM_PLAN(1536, 24, 3, 24, 8, 8)
+TOTEM_PLAN(1600, 20, 3, 20, 20, 4)
+#undef TOTEM_PLAN
+// The window edges above, in four quarters compiled apart (windows_mr_a.cu .. windows_mr_d.cu).
+#define TOTEM_MR_WINDOWS_A(X) X(96) X(320) X(576) X(1152)
+#define TOTEM_MR_WINDOWS_B(X) X(160) X(384) X(640) X(1280)
+#define TOTEM_MR_WINDOWS_C(X) X(192) X(400) X(768) X(1536)
+#define TOTEM_MR_WINDOWS_D(X) X(288) X(448) X(800) X(1600)
+#define TOTEM_MR_WINDOWS(X) TOTEM_MR_WINDOWS_A(X) TOTEM_MR_WINDOWS_B(X) TOTEM_MR_WINDOWS_C(X) TOTEM_MR_WINDOWS_D(X)
+
 template <int N>
 struct Fft {
   static constexpr int P = Plan<N>::P;
   static constexpr int T = N / P;
   static constexpr int stages = Plan<N>::S;
   static constexpr int R0 = Plan<N>::R[0];
-  static constexpr int log2R0 = (R0 == 8) ? 3 : (R0 == 16) ? 4 : 5;
+  static_assert(P % Plan<N>::R[0] == 0 && P % Plan<N>::R[1] == 0 && P % Plan<N>::R[2] == 0, "radices divide P");
+  static_assert(Plan<N>::R[0] * Plan<N>::R[1] * (Plan<N>::S == 3 ? Plan<N>::R[2] : 1) == N, "radices multiply to N");
   // twiddle-table size: sum over stages s >= 1 of Ns * (R_s - 1)
   static constexpr int tw_size = (stages == 2) ? R0 * (Plan<N>::R[1] - 1)
                                                : R0 * (Plan<N>::R[1] - 1) + R0 * Plan<N>::R[1] * (Plan<N>::R[2] - 1);
@@ -262,11 +345,13 @@ struct PadMap {
   // padded index of position p = j + m*T (the register layout of a thread)
   __device__ __forceinline__ static int pos(int j, int m) {
     constexpr int T = Fft<N>::T;
-    if constexpr (T <= R0) {
+    if constexpr (T <= R0 && R0 % T == 0) {
       constexpr int per = R0 / T;  // register slots per R0 block
       return split(m / per, j + (m % per) * T);
-    } else {
+    } else if constexpr (T > R0 && T % R0 == 0) {
       return split(j / R0 + m * (T / R0), j % R0);
+    } else {
+      return pad(j + m * T);  // mixed-radix plans where neither of T, R0 divides the other
     }
   }
 };
@@ -440,10 +525,23 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Launch shapes shared by the kernels that transform whole rows or whole columns.
 // Rows: G transforms of T threads per CTA (each transform inside one warp, or a named barrier
 // per transform when T > 32), at most 32 KB of exchange space per CTA.
+// Rows per CTA: the largest g up to the cap (256 threads, or 4096 elements) that divides N (a
+// CTA's rows belong to one probe) and makes whole warps; for power-of-two N the cap itself.
+template <int N>
+constexpr int row_group_count() {
+  constexpr int T = Fft<N>::T;
+  constexpr int cap = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
+  for (int g = cap > 0 ? cap : 1; g >= 1; --g)
+    if (N % g == 0 && (g * T) % 32 == 0) return g;
+  for (int g = (cap > 0 ? cap : 1) + 1; g <= 64; ++g)
+    if (N % g == 0 && (g * T) % 32 == 0) return g;
+  return 1;
+}
 template <int N, int CTAS = 0>
 struct RowCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
-  static constexpr int G = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
+  static constexpr int G = row_group_count<N>();
+  static_assert((G * T) % 32 == 0 && N % G == 0, "row tile: whole warps, whole probes");
   // resident CTAs of 128 threads requested per SM: 5 caps registers at 96 per thread, which
   // the padded exchange addressing fits without spilling up to N = 1024 (and 5 CTAs is also
   // what the row pass's shared memory allows).  At 1024 a 128-register cap (4 CTAs) made the
@@ -462,6 +560,7 @@ struct ColCfg {
   // GW = 0: the default width, 16 columns (one 128-byte segment per row) up to N = 512, 8 (64
   // bytes) up to 2048 (at 2048 one 512-thread CTA per SM; 4 columns at two CTAs was 10 % slower)
   static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 2048 ? 8 : 2));
+  static_assert((G * T) % 32 == 0 && N % G == 0, "column tile: whole warps, whole tiles");
   // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
 };
@@ -482,10 +581,15 @@ struct BandCols {
   static constexpr int hi = ((N - K) / L * L > lo) ? (N - K) / L * L : lo;
 };
 
+// Transform groups of T threads: within a warp when T divides 32, whole warps with a named barrier
+// when 32 divides T, else (mixed-radix T such as 12 or 20) the whole CTA, whose groups all run
+// the same sequence of barriers.
 template <int N>
 __device__ __forceinline__ auto group_sync(int g) {
-  if constexpr (Fft<N>::T <= 32) return SyncWarp{};
-  else return SyncNamed<Fft<N>::T>{1 + g};
+  constexpr int T = Fft<N>::T;
+  if constexpr (T <= 32 && 32 % T == 0) return SyncWarp{};
+  else if constexpr (T % 32 == 0) return SyncNamed<T>{1 + g};
+  else return SyncBlock{};
 }
 
 // Cooperative copy of the twiddle tables into shared memory (caller synchronises afterwards).

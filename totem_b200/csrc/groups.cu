@@ -3,36 +3,11 @@
 #include <map>
 #include <mutex>
 
-#include "slice_tiles.cuh"
+#include "passes.cuh"
 
 namespace totem {
 
 namespace {
-
-// Row pass of a continuous batch over groups of one window size.
-template <int N>
-__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB)
-    k_row_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
-                 const float2* __restrict__ tw) {
-  constexpr int G = RowCfg<N>::G, per_item = N / G;
-  const int li = blockIdx.x / per_item;
-  const int row0 = (blockIdx.x - li * per_item) * G;
-  const int gidx = find_group(item_begin, ngroups, li);
-  row_group_tile<N>(groups[gidx], li - __ldg(item_begin + gidx), row0, tick, tw);
-}
-
-// Column pass of a continuous batch over groups of one window size.
-template <int N>
-__global__ void __launch_bounds__(ColCfg<N>::G * ColCfg<N>::T, ColCfg<N>::MINB)
-    k_col_groups(const GroupDesc* __restrict__ groups, const int* __restrict__ item_begin, int ngroups, int tick,
-                 const float2* __restrict__ tw, TileSkip skip) {
-  constexpr int G = ColCfg<N>::G, nblk = N / G;
-  const int active = nblk - skip.nskip;
-  const int li = blockIdx.x / active, t = blockIdx.x - li * active;
-  const int cb = t < skip.z0 ? t : t + skip.nskip;
-  const int gidx = find_group(item_begin, ngroups, li);
-  col_group_tile<N, G>(groups[gidx], li - __ldg(item_begin + gidx), cb, tick, tw);
-}
 
 // ---------------------------------------------------------------------------------------------
 // Windows of different sizes in one launch.  A persistent CTA of kMixedThreads threads takes
@@ -101,29 +76,6 @@ __global__ void __launch_bounds__(kMixedThreads, 2)
 
 }  // namespace
 
-template <int N>
-Status row_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
-                  cudaStream_t st) {
-  constexpr int G = RowCfg<N>::G, T = RowCfg<N>::T;
-  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_row_groups<N>, smem));
-  k_row_groups<N><<<(unsigned)(items * (N / G)), G * T, smem, st>>>(groups, item_begin, ngroups, tick, tw);
-  return cuda_status(cudaGetLastError(), "k_row_groups");
-}
-
-template <int N>
-Status col_groups(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick, const float2* tw,
-                  TileSkip skip, cudaStream_t st) {
-  constexpr int G = ColCfg<N>::G, T = ColCfg<N>::T;
-  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_col_groups<N>, smem));
-  if (skip.nskip < 0 || skip.z0 < 0 || skip.z0 + skip.nskip > N / G)
-    return Status::Err(TOTEM_ERR_STATE, "column tiles to skip out of range");
-  k_col_groups<N><<<(unsigned)(items * (N / G - skip.nskip)), G * T, smem, st>>>(groups, item_begin, ngroups, tick,
-                                                                                 tw, skip);
-  return cuda_status(cudaGetLastError(), "k_col_groups");
-}
-
 Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                          const float2* tw, cudaStream_t st) {
   if (items <= 0 || ngroups <= 0) return Status::Ok();
@@ -135,7 +87,8 @@ Status launch_row_groups(int n, const GroupDesc* groups, const int* item_begin, 
     case 1024: return row_groups<1024>(groups, item_begin, ngroups, items, tick, tw, st);
     case 2048: return row_groups<2048>(groups, item_begin, ngroups, items, tick, tw, st);
   }
-  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
+  if (const WindowOps* o = radix_window_ops(n)) return o->row_groups(groups, item_begin, ngroups, items, tick, tw, st);
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching: unsupported window edge");
 }
 
 Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
@@ -149,7 +102,9 @@ Status launch_col_groups(int n, const GroupDesc* groups, const int* item_begin, 
     case 1024: return col_groups<1024>(groups, item_begin, ngroups, items, tick, tw, skip, st);
     case 2048: return col_groups<2048>(groups, item_begin, ngroups, items, tick, tw, skip, st);
   }
-  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching needs a power-of-two window 64..2048");
+  if (const WindowOps* o = radix_window_ops(n))
+    return o->col_groups(groups, item_begin, ngroups, items, tick, tw, skip, st);
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "continuous batching: unsupported window edge");
 }
 
 template <int N>

@@ -14,33 +14,11 @@
 // Layout in HBM: psi[item][row][col] complex64, item = w * depth + pos (probe-major, as the
 // reference's w_series loop); T[slice][P_H][P_W]; H[N][N] and the masks [A][N][N] in natural
 // FFT order (the masks for the exit detector are ifftshift(aper), computed at upload).
-#include "slice_tiles.cuh"
+#include "passes.cuh"
 
 namespace totem {
 
 namespace {
-
-// Column-pass variants, per 2048-probe launch on the SrTiO3 512^2 workload (microseconds per
-// probe): 16-column tiles with the propagator read from global memory (L2-resident) at a
-// 128-register cap, 0.98 (the default); 8-column tiles 1.11; 32-column tiles 1.32; 16-column
-// tiles at an 80-register cap 1.10 (it spills).  A persistent column pass streaming the next
-// tile into shared memory with cp.async while transforming the current one (one 256-thread CTA
-// per SM for its 134 KB of shared memory) measured 1.22, with 8-column tiles (3 CTAs per SM)
-// 1.24: the pass needs warps more than it needs its loads hidden.  With 8-column tiles,
-// prefetching the propagator into shared memory (4.6 ms against 4.3 ms per 4096 probes) and an
-// 80-register cap (5.8 ms) were slower.
-// The launch covers the tiles outside [skip.z0, skip.z0 + skip.nskip) only.
-template <int N, bool PREFETCH, int CTAS128, int GW>
-__global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
-    k_col_pass(SliceLoopArgs a, int flags, TileSkip skip) {
-  constexpr int G = ColCfg<N, CTAS128, GW>::G;
-  constexpr int nblk = N / G;
-  const int active = nblk - skip.nskip;
-  const int item = blockIdx.x / active, t = blockIdx.x - item * active;
-  const int cb = t < skip.z0 ? t : t + skip.nskip;
-  const ColInputs in{a.prop, a.mask_mid, a.mask_exit, a.aper_num, a.part_mid, a.part_exit};
-  col_tile<N, PREFETCH, G>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw);
-}
 
 __global__ void k_det_reduce(const double* __restrict__ part, int nblk, int aper_num, int items, int item0,
                              int depth, double* __restrict__ acc, TileSkip skip) {
@@ -65,69 +43,6 @@ __global__ void k_combine(const double* __restrict__ acc, const double* __restri
   out[i] = s;
 }
 
-template <int N, bool PREFETCH, int CTAS128, int GW>
-Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
-  constexpr int G = ColCfg<N, CTAS128, GW>::G, T = ColCfg<N>::T;
-  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128, GW>, smem));
-  const TileSkip skip = a.skip_band ? band_tiles(N, N / G) : TileSkip();
-  k_col_pass<N, PREFETCH, CTAS128, GW>
-      <<<(unsigned)((long)a.items * (N / G - skip.nskip)), G * T, smem, st>>>(a, flags, skip);
-  TOTEM_TRY(cuda_status(cudaGetLastError(), "k_col_pass"));
-  if ((flags & 8) && skip.nskip) {
-    // a kept spectrum is stored whole: on the skipped columns it is exactly zero (the propagator is)
-    const size_t pitch = (size_t)N * sizeof(float2);
-    TOTEM_CUDA(cudaMemset2DAsync(a.psi + (size_t)skip.z0 * G, pitch, 0, (size_t)skip.nskip * G * sizeof(float2),
-                                 (size_t)a.items * N, st));
-  }
-  return Status::Ok();
-}
-
-// Column-pass variants: 0/1 default; 2 propagator prefetched to shared memory; 3 a cap of
-// 6 x 128 threads per SM (80 registers at 16 columns); 5 tiles of 8 columns (up to N = 2048);
-// 6 tiles of 32 columns (up to N = 512).  col_blocks() gives the number of column tiles, i.e. of
-// detector partial sums per probe, of each variant.
-template <int N>
-Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
-  switch (a.col_variant) {
-    case 2: return col_pass_v<N, true, 4, 0>(a, flags, st);
-    case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4), 0>(a, flags, st);
-    case 5: return col_pass_v<N, false, 4, (N <= 2048 ? 8 : 0)>(a, flags, st);
-    case 6: return col_pass_v<N, false, 4, (N <= 512 ? 32 : 0)>(a, flags, st);
-    default: return col_pass_v<N, false, 4, 0>(a, flags, st);
-  }
-}
-
-template <int N>
-int col_tiles(int variant) {
-  if (N <= 2048 && variant == 5) return N / 8;
-  if (N <= 512 && variant == 6) return N / 32;
-  return N / ColCfg<N>::G;
-}
-
-template <int N, int S>
-void fill_stage(std::vector<float2>& out) {
-  if constexpr (S < Fft<N>::stages) {
-    constexpr int R = StageInfo<N, S>::R, Ns = StageInfo<N, S>::Ns;
-    if constexpr (S >= 1) {
-      for (int r = 1; r < R; ++r)
-        for (int k = 0; k < Ns; ++k) {
-          const long e = (long)k * r * (N / (Ns * R));
-          const double ang = -2.0 * kPi * (double)e / (double)N;
-          out[StageInfo<N, S>::tw_off + (r - 1) * Ns + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
-        }
-    }
-    fill_stage<N, S + 1>(out);
-  }
-}
-
-template <int N>
-std::vector<float2> tables() {
-  std::vector<float2> t(Fft<N>::tw_size > 0 ? Fft<N>::tw_size : 1);
-  fill_stage<N, 0>(t);
-  return t;
-}
-
 }  // namespace
 
 std::vector<float2> stage_twiddles(int n) {
@@ -140,7 +55,24 @@ std::vector<float2> stage_twiddles(int n) {
     case 2048: return tables<2048>();
     case 4096: return tables<4096>();
   }
+  if (const WindowOps* o = radix_window_ops(n)) return o->twiddles();
   return {};
+}
+
+const WindowOps* radix_window_ops_a(int n);
+const WindowOps* radix_window_ops_b(int n);
+const WindowOps* radix_window_ops_c(int n);
+const WindowOps* radix_window_ops_d(int n);
+
+const WindowOps* radix_window_ops(int n) {
+  for (auto f : {radix_window_ops_a, radix_window_ops_b, radix_window_ops_c, radix_window_ops_d})
+    if (const WindowOps* o = f(n)) return o;
+  return nullptr;
+}
+
+bool fused_window_ok(int n) {
+  if (n >= 64 && n <= 2048 && (n & (n - 1)) == 0) return true;
+  return radix_window_ops(n) != nullptr;
 }
 
 int col_blocks(int n, int variant) {
@@ -152,6 +84,7 @@ int col_blocks(int n, int variant) {
     case 1024: return col_tiles<1024>(variant);
     case 2048: return col_tiles<2048>(variant);
   }
+  if (const WindowOps* o = radix_window_ops(n)) return o->col_tiles;  // one tile width for every variant
   return 0;
 }
 
@@ -164,7 +97,8 @@ Status launch_col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
     case 1024: return col_pass<1024>(a, flags, st);
     case 2048: return col_pass<2048>(a, flags, st);
   }
-  return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused slice loop needs a power-of-two window 64..2048");
+  if (const WindowOps* o = radix_window_ops(a.n)) return o->col_pass(a, flags, st);
+  return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused slice loop: unsupported window edge");
 }
 
 Status launch_det_reduce(const double* part, int nblk, int aper_num, int items, int item0, int depth, double* acc,
@@ -181,6 +115,11 @@ void band_columns(int n, int* lo, int* hi) {
   case NN: *lo = BandCols<NN>::lo; *hi = BandCols<NN>::hi; return;
     TOTEM_BAND(64) TOTEM_BAND(128) TOTEM_BAND(256) TOTEM_BAND(512) TOTEM_BAND(1024) TOTEM_BAND(2048)
 #undef TOTEM_BAND
+  }
+  if (const WindowOps* o = radix_window_ops(n)) {
+    *lo = o->band_lo;
+    *hi = o->band_hi;
+    return;
   }
   *lo = *hi = 0;
 }

@@ -39,7 +39,7 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
-bool fused_window(int h, int w) { return h == w && h >= 64 && h <= 2048 && (h & (h - 1)) == 0; }
+bool fused_window(int h, int w) { return h == w && totem::fused_window_ok(h); }
 
 struct Request {
   unsigned long long ticket = 0;
@@ -718,7 +718,7 @@ int totem_server_submit(totem_server* s, const TotemStemArgs* args, TotemStemOut
   Status st = totem_session::validate(args, true);
   if (!st.ok()) return server_fail(st);
   if (args->depth > 0 && !fused_window(args->height, args->width))
-    return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server runs square power-of-two windows of 64..2048"));
+    return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server runs square windows of 64..2048: powers of two or the mixed-radix edges"));
   if (args->depth > 0 && args->slices < 1)
     return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server needs at least one slice"));
   std::unique_ptr<Request> r(new Request());
