@@ -58,8 +58,9 @@ enum { TOTEM_PARAM_PENG = 0,   /* rows of 13 (neutral) / 25 (ionic) columns */
        TOTEM_PARAM_LOBATO = 1  /* rows of 14 / 26 columns                     */ };
 
 /* Slice-loop implementation.  TOTEM_PATH_FUSED runs the hand-written kernels where they apply
- * (square power-of-two windows of 64..2048 for the slice loop, power-of-two potential grids of
- * 64..4096 for the transmission FFT) and cuFFT elsewhere; TotemTiming reports what ran.
+ * (square windows of 64..2048 for the slice loop: powers of two and the mixed-radix edges 96, 160,
+ * 192, 288, 320, 384, 400, 448, 576, 640, 768, 800, 1152, 1280, 1536, 1600; power-of-two potential
+ * grids of 64..4096 for the transmission FFT) and cuFFT elsewhere; TotemTiming reports what ran.
  * TOTEM_PATH_FUSED_ONLY fails with TOTEM_ERR_UNSUPPORTED instead of using cuFFT. */
 enum { TOTEM_PATH_FUSED = 0,      /* shared-memory FFT passes fused with the multiplies and detectors */
        TOTEM_PATH_PLAIN = 1,      /* cuFFT plus separate element-wise kernels (comparator)           */
@@ -385,7 +386,8 @@ TOTEM_API int totem_tcc_stack(const TotemAberrations *ab, double lambda_nm, int 
  *
  * The caller keeps every buffer of ``args`` and ``out`` alive and unmodified until the request is
  * done (totem_server_wait returned or totem_server_info reports DONE / FAILED).  Only the fused
- * path is served: the window must be square, a power of two in [64, 2048], and slices >= 1.
+ * path is served: the window must be square, of an edge the fused slice loop takes (see
+ * TOTEM_PATH_FUSED), and slices >= 1.
  * ------------------------------------------------------------------------------------------- */
 typedef struct totem_server totem_server;
 
