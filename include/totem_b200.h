@@ -317,7 +317,10 @@ TOTEM_API int totem_stem_slices_noalloc(const void *transmission, int p_height, 
  * image.  The reference builds the transmission with the *P MEX and runs this part in MATLAB
  * (ToTEM_submit_v1.m:1259-1369):  psi = incident wave;  per slice  psi = ifft2(fft2(psi .* T_k)
  * .* psf_fft);  exit wave = psi;  image = sum_k gfsf_k |ifft2(fft2(psi) .* tf_k)|^2 with
- * tf_k = ifftshift(tcc_k .* aperture).  The grid must be square, a power of two in [64, 2048].
+ * tf_k = ifftshift(tcc_k .* aperture).  The grid must be square (the reference squares the
+ * potential grid, ToTEM_submit_v1.m:1240-1242).  Edges the fused slice loop takes (TOTEM_PATH_FUSED)
+ * run the fused passes, every other edge cuFFT; totem_session_timing's slice_path says which.  The
+ * bfloat16 transmission trial (t_storage TOTEM_T_BF16) needs a power-of-two edge of 64..2048.
  * ------------------------------------------------------------------------------------------- */
 typedef struct TotemHrtemArgs {
   int struct_size;               /* sizeof(TotemHrtemArgs)                                     */

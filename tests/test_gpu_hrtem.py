@@ -36,6 +36,26 @@ def test_hrtem_vs_oracle(engine_lib, case):
     assert rel_l2(img, rimg) < TOL
 
 
+@pytest.mark.parametrize("p,path", [(192, capi.PATH_FUSED), (400, capi.PATH_FUSED), (200, capi.PATH_PLAIN),
+                                    (250, capi.PATH_PLAIN)])
+def test_hrtem_grid_edges_vs_oracle(engine_lib, p, path):
+    # the reference's HRTEM grid is the potential grid, round(extent / sampling) made even: mixed-radix
+    # edges run the fused passes, every other edge cuFFT, and the session says which ran
+    req, hs = request.build_si_hrtem_001(cells=(3, 3, 2), p=p, slices=6)
+    s = capi.Session()
+    s.upload(req, stem=False)
+    ex, img = s.hrtem(hs)
+    assert s.timing().slice_path == path
+    if path == capi.PATH_PLAIN:
+        with pytest.raises(capi.TotemError) as e:
+            s.hrtem(hs, t_storage=capi.T_BF16)
+        assert e.value.code == capi.ERR_UNSUPPORTED
+    s.close()
+    rex, rimg = _oracle(req, hs)
+    assert rel_l2(ex, rex) < TOL
+    assert rel_l2(img, rimg) < TOL
+
+
 def test_hrtem_session_matches_one_shot_and_bf16_trial(engine_lib):
     req, hs = request.build_si_hrtem_001(cells=(4, 4, 4), p=256, slices=16)
     ex1, img1 = capi.hrtem_run(req, hs)

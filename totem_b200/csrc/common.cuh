@@ -263,6 +263,9 @@ struct WindowOps {
   Status (*col_groups)(const GroupDesc* groups, const int* item_begin, int ngroups, long items, int tick,
                        const float2* tw, TileSkip skip, cudaStream_t st);
   std::vector<float2> (*twiddles)();
+  // HRTEM imaging (launch_exit_wave / launch_tcc_image semantics: out_i == nullptr for the exit wave)
+  Status (*image)(const float2* spec, const float2* tf, int planes, const double* w, float2* work, float2* out_c,
+                  float* out_i, const float2* tw, cudaStream_t st);
 };
 const WindowOps* radix_window_ops(int n);
 
@@ -289,6 +292,11 @@ Status launch_plain_gather_mul(float2* psi, const float2* tslice, int h, int w, 
                                ScanGeom geo, cudaStream_t st);
 Status launch_plain_mul(float2* psi, const float2* m, int vol, int items, cudaStream_t st);
 Status launch_plain_scale(float2* psi, float s, long total, cudaStream_t st);
+// HRTEM on cuFFT: work[k] = spec .* tf[k] for k < planes (vol elements each), and
+// out[e] = sum_k w_k |work[k][e] * s|^2 in ascending k (the order of the fused image kernel).
+Status launch_plain_tf_mul(float2* work, const float2* spec, const float2* tf, int vol, int planes, cudaStream_t st);
+Status launch_plain_image(const float2* work, int planes, const double* w, float s, int vol, float* out,
+                          cudaStream_t st);
 Status launch_plain_detect(const float2* psi, const float* masks, int aper_num, int vol, int items,
                            double* part, int nblk, cudaStream_t st);
 

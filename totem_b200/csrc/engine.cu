@@ -896,10 +896,15 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
     return Status::Err(TOTEM_ERR_INVALID_ARG, "defoci > 0 needs tf_re, tf_im and weights");
   if (hr->t_storage != TOTEM_T_COMPLEX64 && hr->t_storage != TOTEM_T_BF16)
     return Status::Err(TOTEM_ERR_INVALID_ARG, "unknown transmission storage");
-  if (p_h != p_w || !is_pow2(p_h) || p_h < 64 || p_h > 2048 || slices < 1)
-    return Status::Err(TOTEM_ERR_UNSUPPORTED, "HRTEM needs a square power-of-two grid of 64..2048 and a slice");
-  TOTEM_CUDA(cudaSetDevice(device));
+  // the reference squares the potential grid (ToTEM_submit_v1.m:1240-1242); the fused passes take
+  // the edges of fused_window_ok, cuFFT every other edge
+  if (p_h != p_w || p_h < 2 || slices < 1)
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "HRTEM needs a square grid and a slice");
   const int n = p_h;
+  const bool fused = totem::fused_window_ok(n);
+  if (!fused && hr->t_storage != TOTEM_T_COMPLEX64)
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "the bfloat16 transmission trial needs a grid of the fused passes");
+  TOTEM_CUDA(cudaSetDevice(device));
   const size_t vol = (size_t)n * n;
   int launches = 0;
   if (!t_valid) TOTEM_TRY(build_transmission(TOTEM_PATH_FUSED, &launches));
@@ -915,6 +920,10 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
   TOTEM_TRY(upload(hr_wave, wave, stream));
   TOTEM_TRY(upload(hr_prop, prop, stream));
   TOTEM_TRY(psi.ensure(vol * sizeof(float2)));
+  timing.slice_path = fused ? TOTEM_PATH_FUSED : TOTEM_PATH_PLAIN;
+  timing.tx_fft_path = ran_tx_fft;
+  timing.tx_builder = ran_tx_builder;
+  if (!fused) return hrtem_plain(hr, out, static_cast<const float2*>(Tslices));
 
   totem::SliceLoopArgs s;
   s.n = n; s.items = 1; s.item0 = 0;
@@ -960,6 +969,66 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
     TOTEM_TRY(hr_img.ensure(vol * sizeof(float)));
     TOTEM_TRY(totem::launch_tcc_image(n, spec, hr_tf.as<float2>(), K, hr_w.as<double>(), hr_work.as<float2>(),
                                       hr_img.as<float>(), tw_pw.as<float2>(), stream));
+    img_h.resize(vol);
+    TOTEM_CUDA(cudaMemcpyAsync(img_h.data(), hr_img.p, vol * sizeof(float), cudaMemcpyDeviceToHost, stream));
+  }
+  TOTEM_CUDA(cudaStreamSynchronize(stream));
+  for (size_t i = 0; i < exit_h.size(); ++i) {
+    if (out->exit_re) out->exit_re[i] = exit_h[i].x;
+    if (out->exit_im) out->exit_im[i] = exit_h[i].y;
+  }
+  for (size_t i = 0; i < img_h.size(); ++i) out->image[i] = img_h[i];
+  return Status::Ok();
+}
+
+// HRTEM on cuFFT for grid edges the fused passes do not take: the same steps as the fused route
+// (psi = wave .* T_0; per slice FFT2, .* propagator, and except after the last slice IFFT2 / N^2 and
+// .* T_{k+1}), the spectrum of the last slice kept; the exit wave is its IFFT2 / N^2 and the image
+// sum_k w_k |IFFT2(spectrum .* tf_k) / N^2|^2.
+Status totem_session::hrtem_plain(const TotemHrtemArgs* hr, TotemHrtemOut* out, const float2* Tp) {
+  const int n = p_h;
+  const size_t vol = (size_t)n * n;
+  const totem::ScanGeom geo{0, 0, 0, 1, 1, n};
+  cufftHandle one;
+  TOTEM_TRY(plan(n, n, 1, &one));
+  float2* ps = psi.as<float2>();
+  TOTEM_CUDA(cudaMemcpyAsync(ps, hr_wave.p, vol * sizeof(float2), cudaMemcpyDeviceToDevice, stream));
+  for (int k = 0; k < slices; ++k) {
+    TOTEM_TRY(totem::launch_plain_gather_mul(ps, Tp + (size_t)k * vol, n, n, 1, 0, geo, stream));
+    TOTEM_CUFFT(cufftExecC2C(one, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
+    TOTEM_TRY(totem::launch_plain_mul(ps, hr_prop.as<float2>(), (int)vol, 1, stream));
+    if (k < slices - 1) {
+      TOTEM_CUFFT(cufftExecC2C(one, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_INVERSE));
+      TOTEM_TRY(totem::launch_plain_scale(ps, 1.f / (float)vol, (long)vol, stream));
+    }
+  }
+  const float scale = 1.f / ((float)n * (float)n);
+  const bool want_exit = out && (out->exit_re || out->exit_im);
+  const bool want_img = out && out->image && hr->defoci > 0;
+  std::vector<float2> exit_h;
+  std::vector<float> img_h;
+  if (want_exit) {
+    TOTEM_TRY(hr_exit.ensure(vol * sizeof(float2)));
+    TOTEM_CUDA(cudaMemcpyAsync(hr_exit.p, ps, vol * sizeof(float2), cudaMemcpyDeviceToDevice, stream));
+    TOTEM_CUFFT(cufftExecC2C(one, (cufftComplex*)hr_exit.p, (cufftComplex*)hr_exit.p, CUFFT_INVERSE));
+    TOTEM_TRY(totem::launch_plain_scale(hr_exit.as<float2>(), scale, (long)vol, stream));
+    exit_h.resize(vol);
+    TOTEM_CUDA(cudaMemcpyAsync(exit_h.data(), hr_exit.p, vol * sizeof(float2), cudaMemcpyDeviceToHost, stream));
+  }
+  if (want_img) {
+    const int K = hr->defoci;
+    std::vector<float2> tf((size_t)K * vol);
+    for (size_t i = 0; i < tf.size(); ++i) tf[i] = make_float2((float)hr->tf_re[i], (float)hr->tf_im[i]);
+    TOTEM_TRY(upload(hr_tf, tf, stream));
+    TOTEM_TRY(upload(hr_w, std::vector<double>(hr->weights, hr->weights + K), stream));
+    TOTEM_TRY(hr_work.ensure((size_t)K * vol * sizeof(float2)));
+    TOTEM_TRY(hr_img.ensure(vol * sizeof(float)));
+    TOTEM_TRY(totem::launch_plain_tf_mul(hr_work.as<float2>(), ps, hr_tf.as<float2>(), (int)vol, K, stream));
+    cufftHandle planes;
+    TOTEM_TRY(plan(n, n, K, &planes));
+    TOTEM_CUFFT(cufftExecC2C(planes, (cufftComplex*)hr_work.p, (cufftComplex*)hr_work.p, CUFFT_INVERSE));
+    TOTEM_TRY(totem::launch_plain_image(hr_work.as<float2>(), K, hr_w.as<double>(), scale, (int)vol,
+                                        hr_img.as<float>(), stream));
     img_h.resize(vol);
     TOTEM_CUDA(cudaMemcpyAsync(img_h.data(), hr_img.p, vol * sizeof(float), cudaMemcpyDeviceToHost, stream));
   }

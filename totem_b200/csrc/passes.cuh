@@ -2,6 +2,7 @@
 // size by the files that dispatch on it (power-of-two windows: rowpass.cu, multislice.cu,
 // groups.cu; mixed-radix windows: windows_mixed_*.cu).
 #pragma once
+#include "hrtem_kernels.cuh"
 #include "slice_tiles.cuh"
 
 namespace totem {
@@ -218,8 +219,16 @@ Status col_pass_mr(const SliceLoopArgs& a, int flags, cudaStream_t st) {
 
 template <int N>
 const WindowOps* window_ops() {
-  static const WindowOps ops{N,           N / ColCfg<N>::G, BandCols<N>::lo, BandCols<N>::hi, &row_pass_mr_any<N>,
-                             &col_pass_mr<N>, &row_groups<N>,  &col_groups<N>,  &tables<N>};
+  static const WindowOps ops{N,
+                             N / ColCfg<N>::G,
+                             BandCols<N>::lo,
+                             BandCols<N>::hi,
+                             &row_pass_mr_any<N>,
+                             &col_pass_mr<N>,
+                             &row_groups<N>,
+                             &col_groups<N>,
+                             &tables<N>,
+                             &image_n<N>};
   return &ops;
 }
 

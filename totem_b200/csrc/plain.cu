@@ -3,7 +3,8 @@
 // This is the comparator the fused path is timed against; its steps mirror the reference's
 // sequence (cuda_source_lobato.cu:1304-1458): initKernel_W, w_p_pointMul, FFT, w_constM_pointMul,
 // [mid detectors], IFFT, scaler, ..., final FFT, detectors.  Plans are cached by the engine and
-// nothing synchronises between launches.
+// nothing synchronises between launches.  The same kernels (plus the transfer-function multiply
+// and the image sum below) carry HRTEM on grids the fused passes do not take.
 #include "common.cuh"
 
 namespace totem {
@@ -77,6 +78,27 @@ __global__ void k_plain_detect(const float2* __restrict__ psi, const float* __re
   }
 }
 
+__global__ void k_plain_tf_mul(float2* __restrict__ work, const float2* __restrict__ spec,
+                               const float2* __restrict__ tf, int vol, long total) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const float2 v = spec[i % vol], t = tf[i];
+    work[i] = make_float2(v.x * t.x - v.y * t.y, v.x * t.y + v.y * t.x);
+  }
+}
+
+__global__ void k_plain_image(const float2* __restrict__ work, int planes, const double* __restrict__ w, float s,
+                              int vol, float* __restrict__ out) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < vol; e += (long)gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int k = 0; k < planes; ++k) {
+      const float2 v = work[(long)k * vol + e];
+      const float ux = v.x * s, uy = v.y * s;
+      acc = fmaf((float)w[k], fmaf(ux, ux, uy * uy), acc);
+    }
+    out[e] = acc;
+  }
+}
+
 inline int grid_for(long total) { return (int)std::min<long>((total + 255) / 256, 148L * 32); }
 
 }  // namespace
@@ -112,6 +134,20 @@ Status launch_plain_detect(const float2* psi, const float* masks, int aper_num, 
   dim3 grid(nblk, items);
   k_plain_detect<<<grid, 256, 0, st>>>(psi, masks, aper_num, vol, part, nblk);
   return cuda_status(cudaGetLastError(), "k_plain_detect");
+}
+
+Status launch_plain_tf_mul(float2* work, const float2* spec, const float2* tf, int vol, int planes, cudaStream_t st) {
+  const long total = (long)planes * vol;
+  if (total == 0) return Status::Ok();
+  k_plain_tf_mul<<<grid_for(total), 256, 0, st>>>(work, spec, tf, vol, total);
+  return cuda_status(cudaGetLastError(), "k_plain_tf_mul");
+}
+
+Status launch_plain_image(const float2* work, int planes, const double* w, float s, int vol, float* out,
+                          cudaStream_t st) {
+  if (vol == 0) return Status::Ok();
+  k_plain_image<<<grid_for(vol), 256, 0, st>>>(work, planes, w, s, vol, out);
+  return cuda_status(cudaGetLastError(), "k_plain_image");
 }
 
 }  // namespace totem

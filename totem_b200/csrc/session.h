@@ -291,6 +291,7 @@ struct totem_session {
   Status run_graphed(const std::vector<long long>& key, const std::function<Status()>& enqueue, int* launches);
   void drop_graph();
   Status hrtem(const TotemHrtemArgs* h, TotemHrtemOut* out);
+  Status hrtem_plain(const TotemHrtemArgs* hr, TotemHrtemOut* out, const float2* Tp);
   Status run(int what, const TotemRunOptions* opt);
   Status collect_timing();
   Status download(TotemStemOut* out);
