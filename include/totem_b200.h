@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define TOTEM_ABI_VERSION 4
+#define TOTEM_ABI_VERSION 3
 
 /* Status codes.  The reference returns silently or aborts MATLAB (waveCuda.cpp:7-16,
  * cuda_source_lobato.cu:1253-1256); every entry point here returns one of these instead. */
@@ -218,14 +218,6 @@ TOTEM_API int totem_set_slice_graphs(int enable);
  * the propagator the caller passes; results equal those with every column computed.  1 = on
  * (default), 0 = off.  Process-wide; no counterpart in the reference. */
 TOTEM_API int totem_set_band_skip(int enable);
-/* The column pass of the fused slice loop takes the propagator from its separable form where the
- * propagator the caller passes has one -- a phase H[r][c] = hy[r] hx[c] on one interval of rows per
- * column and zero elsewhere, as the reference's exp(-i pi lambda dz |k + tilt|^2) cut to a disc
- * (ToTEM_submit_v1.m:1558-1564) is; checked element by element at upload to 1e-6 -- instead of
- * reading an N x N array for every column tile: a row table in shared memory, one factor and one
- * row interval per column.  The products hy[r] hx[c] round differently from the array in the last
- * bits of FP32.  1 = on (default), 0 = off.  Process-wide; no counterpart in the reference. */
-TOTEM_API int totem_set_separable_propagator(int enable);
 /* Failure injection on the host, for tests of the error paths (no GPU fault is involved): after
  * ``alloc_after`` further device allocations of the engine the next one fails once with
  * TOTEM_ERR_OOM, as if the device were full (-1 = off); every ``prepare_every``-th request a server

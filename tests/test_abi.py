@@ -73,7 +73,7 @@ def test_status_strings(lib):
         s = lib.totem_status_string(code).decode()
         assert s and s != "unknown status"
     assert lib.totem_status_string(99).decode() == "unknown status"
-    assert lib.totem_abi_version() == 4
+    assert lib.totem_abi_version() == 3
 
 
 def _has_gpu():

@@ -56,20 +56,6 @@ def test_hrtem_grid_edges_vs_oracle(engine_lib, p, path):
     assert rel_l2(img, rimg) < TOL
 
 
-def test_hrtem_separable_propagator(engine_lib):
-    # the HRTEM propagator (1/2-of-Nyquist disc) in separable form: FP32 rounding apart, the same
-    req, hs = request.build_si_hrtem_001(cells=(4, 4, 2), p=256, slices=8)
-    out = {}
-    for sep in (False, True):
-        capi.set_separable_propagator(sep)
-        try:
-            out[sep] = capi.hrtem_run(req, hs)
-        finally:
-            capi.set_separable_propagator(True)
-    assert rel_l2(out[True][0], out[False][0]) < 1e-6
-    assert rel_l2(out[True][1], out[False][1]) < 1e-6
-
-
 def test_hrtem_session_matches_one_shot_and_bf16_trial(engine_lib):
     req, hs = request.build_si_hrtem_001(cells=(4, 4, 4), p=256, slices=16)
     ex1, img1 = capi.hrtem_run(req, hs)

@@ -283,46 +283,3 @@ def test_mixed_radix_zero_band_skip_and_server(engine_lib, n, p):
     np.testing.assert_array_equal(r1, outs[True][0])
     np.testing.assert_array_equal(m1, outs[True][1])
     _check(req, *outs[True], T=capi.transmission_run(req) if p > 1024 else None)
-
-
-def _runs_sep(req, sep_states=(False, True)):
-    outs = {}
-    for sep in sep_states:
-        capi.set_separable_propagator(sep)
-        try:
-            outs[sep] = capi.stem_run(req)
-        finally:
-            capi.set_separable_propagator(True)
-    return outs
-
-
-@pytest.mark.parametrize("n,p,focal,tilt", [(256, 512, 1, 0.0), (512, 1024, 3, 0.0), (400, 448, 1, 0.0),
-                                             (256, 512, 1, 8.0)])
-def test_separable_propagator_matches_the_array(engine_lib, n, p, focal, tilt):
-    # The reference's propagator, a phase cut to a disc (shifted by a beam tilt), is separable on
-    # per-column row intervals: the column pass builds it from a row table and a column factor
-    # instead of reading the N x N array.  The two forms differ in FP32 rounding only.
-    from dataclasses import replace
-    from totem_b200 import optics
-    req = request.build_small_stem(n=n, p=p, raster=(2, 2), step=9, slices=4, sampling=max(0.05, 20.0 / p),
-                                   cells=4, mid_layer=(2,), focal_steps=focal)
-    if tilt:
-        req = replace(req, prop=optics.propagator(n, max(0.05, 20.0 / p), 200.0, 1.9525, "2/3", tilt_mrad=tilt,
-                                                  tilt_deg=30.0))
-    outs = _runs_sep(req)
-    for a, b in zip(outs[False], outs[True]):
-        assert rel_l2(b, a) < 1e-6, rel_l2(b, a)
-    _check(req, *outs[True])
-
-
-def test_non_separable_propagator_reads_the_array(engine_lib):
-    # a propagator that is not a separable phase (perturbed entry by entry) keeps the array path:
-    # results do not depend on the switch, and match the oracle on the propagator as given
-    from dataclasses import replace
-    req = request.build_small_stem(n=128, p=256, raster=(2, 2), step=9, slices=4, sampling=0.1, mid_layer=(2,))
-    rng = np.random.default_rng(3)
-    req = replace(req, prop=req.prop * (1.0 + 1e-3 * rng.standard_normal(req.prop.shape)))
-    outs = _runs_sep(req)
-    for a, b in zip(outs[False], outs[True]):
-        np.testing.assert_array_equal(a, b)
-    _check(req, *outs[True])

@@ -154,7 +154,6 @@ def load() -> C.CDLL:
     lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
     lib.totem_set_slice_graphs.argtypes = [C.c_int]
     lib.totem_set_band_skip.argtypes = [C.c_int]
-    lib.totem_set_separable_propagator.argtypes = [C.c_int]
     lib.totem_inject_failures.argtypes = [C.c_longlong, C.c_int]
     lib.totem_load_tuning.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
     lib.totem_tuned_config.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -173,7 +172,7 @@ def load() -> C.CDLL:
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
-                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_set_separable_propagator", "totem_inject_failures", "totem_load_tuning", "totem_tuned_config", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
+                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_inject_failures", "totem_load_tuning", "totem_tuned_config", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -577,12 +576,6 @@ def inject_failures(alloc_after: int = -1, prepare_every: int = 0):
 def set_band_skip(enable: bool):
     """``totem_set_band_skip``: skip the wave columns the propagator zeroes (default on)."""
     check(load().totem_set_band_skip(1 if enable else 0))
-
-
-def set_separable_propagator(enable: bool):
-    """``totem_set_separable_propagator``: build the column pass's propagator from its separable
-    form where it has one (default on)."""
-    check(load().totem_set_separable_propagator(1 if enable else 0))
 
 
 def set_slice_graphs(enable: bool):

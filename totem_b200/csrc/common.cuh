@@ -172,15 +172,6 @@ bool band_skip_ok(int n, int band, int col_variant);
 TileSkip band_tiles(int n, int nblk);
 // Process-wide: skip the zero band where band_skip_ok (totem_set_band_skip; on by default).
 bool band_skip_enabled();
-// A propagator H [n][n] (FFT order) that is a separable phase on a per-column interval of rows, as
-// the reference's exp(-i pi lambda dz |k + tilt|^2) cut to a disc (ToTEM_submit_v1.m:1558-1564) is:
-// H[r][c] = hy[r] * hx[c] when the centred row index u = (r + n/2) mod n lies in
-// [rows[c].x, rows[c].y), and 0 otherwise, to 1e-6 of |H| on every element.  Fills the three
-// tables (FP32) and returns true when H has that form; checked exactly, element by element.
-bool separable_propagator(const double* re, const double* im, int n, std::vector<float2>* hy,
-                          std::vector<float2>* hx, std::vector<int2>* rows);
-// Process-wide: use the separable form where it holds (totem_set_separable_propagator; default on).
-bool separable_prop_enabled();
 // Host-side failure injection (totem_inject_failures): true when the next device allocation of
 // the engine, or the next server preparation, is to fail (each call counts one event).
 bool inject_alloc_failure();
@@ -195,12 +186,6 @@ struct SliceLoopArgs {
   float2* psi = nullptr;           // [items][N][N]
   const float2* probe = nullptr;   // [w_num][N][N]
   const float2* prop = nullptr;    // [N][N]
-  // the propagator in separable form (prop_hy != nullptr; separable_propagator): H[r][c] =
-  // prop_hy[r] * prop_hx[c] for rows r whose centred index (r + N/2) mod N lies in
-  // [prop_rows[c].x, prop_rows[c].y), else 0; the column pass then reads no H array
-  const float2* prop_hy = nullptr; // [N]
-  const float2* prop_hx = nullptr; // [N]
-  const int2* prop_rows = nullptr; // [N]
   const float2* tw = nullptr;      // N twiddles
   int aper_num = 0;
   const float* mask_mid = nullptr; // [A][N][N] (natural FFT order)

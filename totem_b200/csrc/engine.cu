@@ -12,7 +12,6 @@
 #include <dlfcn.h>
 
 #include <algorithm>
-#include <complex>
 #include <atomic>
 #include <cctype>
 #include <fstream>
@@ -44,7 +43,6 @@ thread_local std::string g_last_error;
 std::atomic<int> g_tx_mode{TOTEM_TX_AUTO};
 std::atomic<int> g_slice_graphs{1};
 std::atomic<int> g_band_skip{1};
-std::atomic<int> g_separable_prop{1};
 std::atomic<long long> g_fail_alloc_after{-1};  // allocations to let through before one fails; -1 off
 std::atomic<long long> g_fail_prepare_every{0};  // every k-th server preparation fails; 0 off
 std::atomic<long long> g_prepares{0};
@@ -242,51 +240,6 @@ void totem::set_last_error(const std::string& msg) { g_last_error = msg; }
 int totem::tx_builder_mode() { return g_tx_mode.load(); }
 bool totem::slice_graphs_enabled() { return g_slice_graphs.load() != 0; }
 bool totem::band_skip_enabled() { return g_band_skip.load() != 0; }
-bool totem::separable_prop_enabled() { return g_separable_prop.load() != 0; }
-
-bool totem::separable_propagator(const double* re, const double* im, int n, std::vector<float2>* hy,
-                                 std::vector<float2>* hx, std::vector<int2>* rows) {
-  if (n < 2 || (n & 1)) return false;
-  using cd = std::complex<double>;
-  auto H = [&](int r, int c) { return cd(re[(size_t)r * n + c], im[(size_t)r * n + c]); };
-  // reference row and column: the ones with the most non-zero entries
-  std::vector<int> row_nz(n, 0), col_nz(n, 0);
-  for (int r = 0; r < n; ++r)
-    for (int c = 0; c < n; ++c)
-      if (H(r, c) != cd(0, 0)) {
-        ++row_nz[r];
-        ++col_nz[c];
-      }
-  const int r0 = (int)(std::max_element(row_nz.begin(), row_nz.end()) - row_nz.begin());
-  const int c0 = (int)(std::max_element(col_nz.begin(), col_nz.end()) - col_nz.begin());
-  const cd h0 = H(r0, c0);
-  if (h0 == cd(0, 0)) return false;
-  std::vector<cd> y(n), x(n);
-  for (int r = 0; r < n; ++r) y[r] = H(r, c0);
-  for (int c = 0; c < n; ++c) x[c] = H(r0, c) / h0;
-  rows->assign(n, make_int2(0, 0));
-  for (int c = 0; c < n; ++c) {
-    // the non-zero rows of column c: one interval [lo, hi) of centred indices u = (r + n/2) mod n
-    int lo = -1, hi = -1;
-    for (int u = 0; u < n; ++u) {
-      const int r = (u + n / 2) % n;
-      const cd v = H(r, c);
-      if (v == cd(0, 0)) {
-        if (lo >= 0 && hi < 0) hi = u;
-        continue;
-      }
-      if (hi >= 0) return false;  // a second interval
-      if (lo < 0) lo = u;
-      if (y[r] == cd(0, 0) || std::abs(v - y[r] * x[c]) > 1e-6 * std::abs(v)) return false;
-    }
-    if (lo >= 0) (*rows)[c] = make_int2(lo, hi < 0 ? n : hi);
-  }
-  hy->resize(n);
-  hx->resize(n);
-  for (int r = 0; r < n; ++r) (*hy)[r] = make_float2((float)y[r].real(), (float)y[r].imag());
-  for (int c = 0; c < n; ++c) (*hx)[c] = make_float2((float)x[c].real(), (float)x[c].imag());
-  return true;
-}
 
 bool totem::inject_alloc_failure() {
   long long left = g_fail_alloc_after.load();
@@ -491,16 +444,6 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
     TOTEM_TRY(upload(probe, pr, st));
     TOTEM_TRY(upload(prop, hp, st));
     band = (h == w) ? totem::spectral_band(a->prop_re, a->prop_im, h, w) : (1 << 30);
-    {
-      std::vector<float2> hy, hx;
-      std::vector<int2> rows;
-      prop_sep = h == w && totem::separable_propagator(a->prop_re, a->prop_im, h, &hy, &hx, &rows);
-      if (prop_sep) {
-        TOTEM_TRY(upload(prop_hy, hy, st));
-        TOTEM_TRY(upload(prop_hx, hx, st));
-        TOTEM_TRY(upload(prop_rows, rows, st));
-      }
-    }
     // exit detector: ifftshift(aper) (the reference shifts the wave instead, cuda_source_lobato.cu:1415)
     std::vector<float> me(vol * std::max(aper_num, 1)), mm;
     for (int q = 0; q < aper_num; ++q)
@@ -743,8 +686,6 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
   const bool skip_band = fused && totem::band_skip_enabled() && t_storage == TOTEM_T_COMPLEX64 &&
                          totem::band_skip_ok(h, band, col_variant);
   const totem::TileSkip skip = skip_band ? totem::band_tiles(h, nblk) : totem::TileSkip();
-  // the column pass builds the propagator from its separable form where it has one
-  const bool use_sep = fused && prop_sep && totem::separable_prop_enabled();
   TOTEM_TRY(psi.ensure((size_t)B * vol * sizeof(float2)));
   TOTEM_TRY(part.ensure((size_t)n_events * B * aper_num * nblk * sizeof(double)));
   TOTEM_TRY(acc.ensure((size_t)n_events * w_num * ad * sizeof(double)));
@@ -777,11 +718,6 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
         s.t_bf16 = (t_storage == TOTEM_T_BF16);
         s.skip_band = skip_band ? 1 : 0;
         s.row_variant = row_variant;
-        if (use_sep) {
-          s.prop_hy = prop_hy.as<float2>();
-          s.prop_hx = prop_hx.as<float2>();
-          s.prop_rows = prop_rows.as<int2>();
-        }
         TOTEM_TRY(prof_begin());
         TOTEM_TRY(totem::launch_row_pass(s, tslice(0), true, stream));
         TOTEM_TRY(prof_end(0));
@@ -849,7 +785,7 @@ Status totem_session::slice_loop(int path, int batch, int col_variant, int t_sto
     // what the launches embed: sizes, buffer addresses and the detection events
     std::vector<long long> key = {h, items_total, B, slices, col_variant, t_storage, n_events, exit_event, aper_num,
                                   w_num, depth, nblk, L, p_h, p_w, begin_row, begin_col, step, width_red,
-                                  (long long)tslice_bytes, skip_band ? 1 : 0, row_variant, use_sep ? 1 : 0};
+                                  (long long)tslice_bytes, skip_band ? 1 : 0, row_variant};
     for (const void* q : {(const void*)psi.p, (const void*)part.p, (const void*)acc.p, (const void*)probe.p,
                           (const void*)prop.p, (const void*)tw_n.p, (const void*)mask_mid.p, (const void*)mask_exit.p,
                           Tslices, (const void*)gfsf_d.p, (const void*)out_result.p, (const void*)out_mid.p})
@@ -1003,19 +939,6 @@ Status totem_session::hrtem(const TotemHrtemArgs* hr, TotemHrtemOut* out) {
                  totem::band_skip_ok(n, totem::spectral_band(hr->prop_re, hr->prop_im, n, n), 0))
                     ? 1
                     : 0;
-  {
-    std::vector<float2> hy, hx;
-    std::vector<int2> rows;
-    hr_sep = totem::separable_propagator(hr->prop_re, hr->prop_im, n, &hy, &hx, &rows);
-    if (hr_sep && totem::separable_prop_enabled()) {
-      TOTEM_TRY(upload(hr_hy, hy, stream));
-      TOTEM_TRY(upload(hr_hx, hx, stream));
-      TOTEM_TRY(upload(hr_rows, rows, stream));
-      s.prop_hy = hr_hy.as<float2>();
-      s.prop_hx = hr_hx.as<float2>();
-      s.prop_rows = hr_rows.as<int2>();
-    }
-  }
   auto tslice = [&](int k) { return static_cast<const char*>(Tslices) + (size_t)k * tslice_bytes; };
   // psi = wave .* T_0, then per slice FFT2 .* psf_fft IFFT2 .* T_{k+1}; the last column pass keeps
   // the spectrum FFT2(psi_{S-1} .* T) .* psf_fft, whose IFFT2 is the exit wave
@@ -1466,13 +1389,6 @@ int totem_inject_failures(long long alloc_after, int prepare_every) {
   g_fail_alloc_after.store(alloc_after);
   g_fail_prepare_every.store(prepare_every);
   g_prepares.store(0);
-  g_last_error.clear();
-  return TOTEM_OK;
-}
-
-int totem_set_separable_propagator(int enable) {
-  if (enable != 0 && enable != 1) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "enable must be 0 or 1"));
-  g_separable_prop.store(enable);
   g_last_error.clear();
   return TOTEM_OK;
 }

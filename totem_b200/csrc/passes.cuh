@@ -73,9 +73,8 @@ Status row_pass(const SliceLoopArgs& a, const void* tslice, cudaStream_t st) {
 // 1.24: the pass needs warps more than it needs its loads hidden.  With 8-column tiles,
 // prefetching the propagator into shared memory (4.6 ms against 4.3 ms per 4096 probes) and an
 // 80-register cap (5.8 ms) were slower.
-// The launch covers the tiles outside [skip.z0, skip.z0 + skip.nskip) only.  SEP: the propagator
-// from its separable form (a.prop_hy ..), no N x N array read.
-template <int N, bool PREFETCH, int CTAS128, int GW, bool SEP = false>
+// The launch covers the tiles outside [skip.z0, skip.z0 + skip.nskip) only.
+template <int N, bool PREFETCH, int CTAS128, int GW>
 __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128, GW>::T, ColCfg<N, CTAS128, GW>::MINB)
     k_col_pass(SliceLoopArgs a, int flags, TileSkip skip) {
   constexpr int G = ColCfg<N, CTAS128, GW>::G;
@@ -83,18 +82,17 @@ __global__ void __launch_bounds__(ColCfg<N, CTAS128, GW>::G * ColCfg<N, CTAS128,
   const int active = nblk - skip.nskip;
   const int item = blockIdx.x / active, t = blockIdx.x - item * active;
   const int cb = t < skip.z0 ? t : t + skip.nskip;
-  const ColInputs in{a.prop,      a.mask_mid, a.mask_exit, a.aper_num, a.part_mid,
-                     a.part_exit, a.prop_hy,  a.prop_hx,   a.prop_rows};
-  col_tile<N, PREFETCH, G, SEP>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw);
+  const ColInputs in{a.prop, a.mask_mid, a.mask_exit, a.aper_num, a.part_mid, a.part_exit};
+  col_tile<N, PREFETCH, G>(a.psi + (long)item * N * N, in, item, cb, flags, a.tw);
 }
 
-template <int N, bool PREFETCH, int CTAS128, int GW, bool SEP = false>
+template <int N, bool PREFETCH, int CTAS128, int GW>
 Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
   constexpr int G = ColCfg<N, CTAS128, GW>::G, T = ColCfg<N>::T;
-  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G) + col_extra_smem<N, SEP>());
-  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128, GW, SEP>, smem));
+  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
+  TOTEM_TRY(ensure_smem((const void*)k_col_pass<N, PREFETCH, CTAS128, GW>, smem));
   const TileSkip skip = a.skip_band ? band_tiles(N, N / G) : TileSkip();
-  k_col_pass<N, PREFETCH, CTAS128, GW, SEP>
+  k_col_pass<N, PREFETCH, CTAS128, GW>
       <<<(unsigned)((long)a.items * (N / G - skip.nskip)), G * T, smem, st>>>(a, flags, skip);
   TOTEM_TRY(cuda_status(cudaGetLastError(), "k_col_pass"));
   if ((flags & 8) && skip.nskip) {
@@ -110,18 +108,8 @@ Status col_pass_v(const SliceLoopArgs& a, int flags, cudaStream_t st) {
 // 6 x 128 threads per SM (80 registers at 16 columns); 5 tiles of 8 columns (up to N = 2048);
 // 6 tiles of 32 columns (up to N = 512).  col_blocks() gives the number of column tiles, i.e. of
 // detector partial sums per probe, of each variant.
-// With the separable propagator (a.prop_hy) variant 2 has nothing to prefetch and runs as the
-// default.
 template <int N>
 Status col_pass(const SliceLoopArgs& a, int flags, cudaStream_t st) {
-  if (a.prop_hy) {
-    switch (a.col_variant) {
-      case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4), 0, true>(a, flags, st);
-      case 5: return col_pass_v<N, false, 4, (N <= 2048 ? 8 : 0), true>(a, flags, st);
-      case 6: return col_pass_v<N, false, 4, (N <= 512 ? 32 : 0), true>(a, flags, st);
-      default: return col_pass_v<N, false, 4, 0, true>(a, flags, st);
-    }
-  }
   switch (a.col_variant) {
     case 2: return col_pass_v<N, true, 4, 0>(a, flags, st);
     case 3: return col_pass_v<N, false, (N <= 1024 ? 6 : 4), 0>(a, flags, st);
@@ -226,7 +214,6 @@ Status row_pass_mr_any(const SliceLoopArgs& a, const void* tslice, bool first, c
 
 template <int N>
 Status col_pass_mr(const SliceLoopArgs& a, int flags, cudaStream_t st) {
-  if (a.prop_hy) return col_pass_v<N, false, 4, 0, true>(a, flags, st);
   return col_pass_v<N, false, 4, 0>(a, flags, st);
 }
 

@@ -185,9 +185,6 @@ struct totem_session {
   bool tb_valid = false;
   // HRTEM inputs and outputs
   totem::DevBuf hr_wave, hr_prop, hr_tf, hr_w, hr_work, hr_exit, hr_img;
-  // the separable form of the STEM propagator (prop_sep) and of the last HRTEM one (hr_sep)
-  totem::DevBuf prop_hy, prop_hx, prop_rows, hr_hy, hr_hx, hr_rows;
-  bool prop_sep = false, hr_sep = false;
   bool t_valid = false;
   bool has_result = false;
   int last_what = 0;

@@ -134,37 +134,23 @@ struct ColInputs {
   int aper_num;
   double* part_mid;   // [items][aper_num][nblk] when flags & 1
   double* part_exit;  // [items][aper_num][nblk] when flags & 2
-  const float2* hy = nullptr;  // the separable form of prop (SliceLoopArgs::prop_hy ..)
-  const float2* hx = nullptr;
-  const int2* rows = nullptr;
 };
-
-// Shared memory of a column tile beyond the twiddles and the exchange region: the separable
-// propagator's row table (SEP).
-template <int N, bool SEP>
-constexpr int col_extra_smem() { return SEP ? N : 0; }
 
 // One CTA's share of a column pass: columns cb*G .. cb*G+G-1 of one probe's wave.  ``item`` is
 // the item's index in the partial-sum arrays.  flags: 1 mid detectors, 2 exit detectors,
-// 4 final pass (no inverse transform), 8 (with 4) store the spectrum.  SEP: the propagator comes
-// from its separable form (row table staged in shared memory, one column factor and row interval
-// per thread) instead of an N x N array.
-template <int N, bool PREFETCH, int G, bool SEP = false>
+// 4 final pass (no inverse transform), 8 (with 4) store the spectrum.
+template <int N, bool PREFETCH, int G>
 __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const ColInputs& in, int item, int cb, int flags,
                                          const float2* __restrict__ tw) {
   constexpr int P = ColCfg<N>::P, T = ColCfg<N>::T;
-  static_assert(!(SEP && PREFETCH), "the separable form needs no prefetch");
   extern __shared__ float2 sh[];
   float2* s_tw = sh;
   float2* s_x = sh + Fft<N>::tw_size;
-  float2* s_hy = s_x + ColLayout<N, G>::size(G);  // SEP: [N]
   __shared__ double red[32];
   constexpr int nblk = N / G;
   const int j = threadIdx.x / G, g = threadIdx.x - j * G;
   const int c = cb * G + g;
   load_twiddles<N>(s_tw, tw);
-  if constexpr (SEP)
-    for (int i = threadIdx.x; i < N; i += blockDim.x) s_hy[i] = __ldg(in.hy + i);
   float2* base = psi_item + c;
   float2 v[P];
 #pragma unroll
@@ -174,17 +160,7 @@ __device__ __forceinline__ void col_tile(float2* __restrict__ psi_item, const Co
   const SyncBlock sync;
   // PREFETCH: the propagator column is copied into the exchange region once the forward
   // transform has finished with it (each thread copies and reads only its own elements)
-  if constexpr (SEP) {
-    const float2 hxc = __ldg(in.hx + c);
-    const int2 iv = __ldg(in.rows + c);
-    fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-      const int r = j + m * T;
-      const int u = r < N / 2 ? r + N / 2 : r - N / 2;  // centred row index
-      v[m] = (u >= iv.x && u < iv.y) ? cmul(cmul(v[m], s_hy[r]), hxc) : make_float2(0.f, 0.f);
-    }
-  } else if constexpr (!PREFETCH) {
+  if constexpr (!PREFETCH) {
     fft_regs<N, false>(v, j, g, s_tw, s_x, L, sync);
 #pragma unroll
     for (int m = 0; m < P; ++m) v[m] = cmul(v[m], __ldg(in.prop + (long)(j + m * T) * N + c));
