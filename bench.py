@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -389,6 +390,18 @@ def main():
                     "probes_per_launch": tm.batch,
                     "transmission_ms": tm.transmission_ms, "slice_loop_ms": tm.slice_loop_ms}
 
+    # the compute-side ceiling: algorithmic FFT flops (two 2-D transforms, 5 N^2 log2 N^2 each, and
+    # 14 N^2 for the multiplies) over the same pass time, against the measured FP32 FMA throughput
+    compute = None
+    if roofline is not None and rank == 0:
+        ffma, ffma2 = capi.fp32_peak(local)
+        flops_ps = 2 * 5 * n2 * math.log2(n2) + 14 * n2
+        achieved_tf = flops_ps * sess.req.probe_slices / (step_ms / 1000.0) / 1e12
+        peak_tf = max(ffma, ffma2)
+        compute = {"bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                   "frac": achieved_tf / peak_tf, "peak_source": "measured FFMA / FFMA2 chains (totem_fp32_peak)",
+                   "ffma_tflops": ffma, "ffma2_tflops": ffma2, "algorithmic_flops_per_probe_slice": flops_ps}
+
     # end to end through the C ABI with host buffers
     e2e = None
     if not ns.no_e2e:
@@ -430,7 +443,7 @@ def main():
             "dtype": "f32 (complex64; FP64 detector sums)",
             "data": "synthetic (seeded SrTiO3 supercell, random-free probe)",
             "config": workload_config(ns, req), "batch": batch_used,
-            "gpu_launches": launches * ns.steps, "clocks": clk.summary(), "roofline": roofline,
+            "gpu_launches": launches * ns.steps, "clocks": clk.summary(), "roofline": roofline, "compute": compute,
             "e2e": e2e, "cpu_baseline": cpu, "plain_cufft": plain, "serving": serve,
         }
         if serve:

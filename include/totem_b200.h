@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define TOTEM_ABI_VERSION 3
+#define TOTEM_ABI_VERSION 4
 
 /* Status codes.  The reference returns silently or aborts MATLAB (waveCuda.cpp:7-16,
  * cuda_source_lobato.cu:1253-1256); every entry point here returns one of these instead. */
@@ -160,6 +160,11 @@ typedef struct TotemTiming {
 typedef struct totem_session totem_session;
 
 TOTEM_API int totem_abi_version(void);
+/* Measured FP32 FMA throughput of GPU ``device`` in TFLOP/s (2 flops per FMA): chains of scalar
+ * FFMA and of packed FFMA2 (two FMAs per instruction), 8 independent chains per thread at full
+ * occupancy, the best of 3 CUDA-event-timed launches after a warm-up (a few ms each).  The
+ * compute-side ceiling of the fused passes, reported beside the HBM roofline. */
+TOTEM_API int totem_fp32_peak(int device, double *ffma_tflops, double *ffma2_tflops);
 TOTEM_API const char *totem_status_string(int status);
 /* Message describing the last failure on the calling thread ("" if none). */
 TOTEM_API const char *totem_last_error(void);

@@ -73,7 +73,7 @@ def test_status_strings(lib):
         s = lib.totem_status_string(code).decode()
         assert s and s != "unknown status"
     assert lib.totem_status_string(99).decode() == "unknown status"
-    assert lib.totem_abi_version() == 3
+    assert lib.totem_abi_version() == 4
 
 
 def _has_gpu():
@@ -94,10 +94,13 @@ def test_no_device_is_an_error_not_a_crash(lib):
     assert "device" in lib.totem_last_error().decode().lower()
     h = C.c_void_p()
     assert lib.totem_session_create(-1, None, C.byref(h)) == capi.ERR_NO_DEVICE
+    a, b = C.c_double(), C.c_double()
+    assert lib.totem_fp32_peak(0, C.byref(a), C.byref(b)) == capi.ERR_NO_DEVICE
 
 
 def test_null_arguments_are_rejected(lib):
     assert lib.totem_session_create(0, None, None) == capi.ERR_INVALID_ARG
+    assert lib.totem_fp32_peak(0, None, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_upload(None, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_run(None, 0, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_destroy(None) == capi.OK

@@ -67,3 +67,14 @@ def test_engine_applies_the_table(engine_lib, tmp_path):
         np.testing.assert_allclose(mid, mid2, rtol=1e-12)
     finally:
         capi.load_tuning(capi.TUNING_FILE)
+
+
+def test_fp32_peak_is_measured(engine_lib):
+    # B200: 148 SMs x 128 FP32 lanes x 2 flops at 1.3-2.0 GHz, i.e. about 50-75 TFLOP/s of scalar
+    # FFMA; packed FFMA2 at most twice that
+    ffma, ffma2 = capi.fp32_peak(0)
+    assert 20.0 < ffma < 200.0, ffma
+    assert 20.0 < ffma2 < 400.0, ffma2
+    with pytest.raises(capi.TotemError) as e:
+        capi.fp32_peak(99)
+    assert e.value.code == capi.ERR_INVALID_ARG

@@ -154,6 +154,7 @@ def load() -> C.CDLL:
     lib.totem_set_tx_builder.argtypes = [C.c_int, C.c_size_t]
     lib.totem_set_slice_graphs.argtypes = [C.c_int]
     lib.totem_set_band_skip.argtypes = [C.c_int]
+    lib.totem_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.totem_inject_failures.argtypes = [C.c_longlong, C.c_int]
     lib.totem_load_tuning.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
     lib.totem_tuned_config.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -172,7 +173,7 @@ def load() -> C.CDLL:
                  "totem_hrtem_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
-                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_inject_failures", "totem_load_tuning", "totem_tuned_config", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
+                 "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_fp32_peak", "totem_inject_failures", "totem_load_tuning", "totem_tuned_config", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib
@@ -571,6 +572,13 @@ def inject_failures(alloc_after: int = -1, prepare_every: int = 0):
     """``totem_inject_failures``: make the next device allocation after ``alloc_after`` more fail
     once (-1 = off), and every ``prepare_every``-th server preparation fail (0 = off)."""
     check(load().totem_inject_failures(int(alloc_after), int(prepare_every)))
+
+
+def fp32_peak(device: int = 0):
+    """``totem_fp32_peak``: measured FP32 FMA throughput of a GPU in TFLOP/s, (scalar, packed)."""
+    a, b = C.c_double(), C.c_double()
+    check(load().totem_fp32_peak(int(device), C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def set_band_skip(enable: bool):

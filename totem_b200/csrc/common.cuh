@@ -172,6 +172,8 @@ bool band_skip_ok(int n, int band, int col_variant);
 TileSkip band_tiles(int n, int nblk);
 // Process-wide: skip the zero band where band_skip_ok (totem_set_band_skip; on by default).
 bool band_skip_enabled();
+// Measured FP32 FMA throughput of ``device`` in TFLOP/s (2 flops per FMA), scalar and packed.
+Status measure_fma_rates(int device, double* ffma_tflops, double* ffma2_tflops);
 // Host-side failure injection (totem_inject_failures): true when the next device allocation of
 // the engine, or the next server preparation, is to fail (each call counts one event).
 bool inject_alloc_failure();

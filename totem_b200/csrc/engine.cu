@@ -1238,6 +1238,17 @@ extern "C" {
 
 int totem_abi_version(void) { return TOTEM_ABI_VERSION; }
 
+int totem_fp32_peak(int device, double* ffma_tflops, double* ffma2_tflops) {
+  if (!ffma_tflops || !ffma2_tflops) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "output pointer is NULL"));
+  return guarded([&]() -> Status {
+    int count = 0;
+    const cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return Status::Err(TOTEM_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= count) return Status::Err(TOTEM_ERR_INVALID_ARG, "device index out of range");
+    return totem::measure_fma_rates(device, ffma_tflops, ffma2_tflops);
+  });
+}
+
 const char* totem_status_string(int status) {
   switch (status) {
     case TOTEM_OK: return "ok";

@@ -98,4 +98,76 @@ Status launch_to_bf16(const float2* in, void* out, long n, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_to_bf16");
 }
 
+namespace {
+
+// FP32 FMA throughput: every thread runs kFmaChains independent chains a = a * m + c, scalar (FFMA)
+// or on packed pairs (FFMA2, __ffma2_rn, two FMAs per instruction); with m = 0.999, c = 0.001 the
+// values stay near 1.  The sum is stored so that nothing is dead code.
+constexpr int kFmaChains = 8;
+
+__global__ void k_fma_rate(float* __restrict__ out, int iters) {
+  float a[kFmaChains];
+#pragma unroll
+  for (int i = 0; i < kFmaChains; ++i) a[i] = 1.f + 1e-3f * i + 1e-7f * threadIdx.x;
+  for (int it = 0; it < iters; ++it)
+#pragma unroll
+    for (int i = 0; i < kFmaChains; ++i) a[i] = fmaf(a[i], 0.999f, 0.001f);
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < kFmaChains; ++i) s += a[i];
+  out[(long)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__global__ void k_fma2_rate(float* __restrict__ out, int iters) {
+  float2 a[kFmaChains];
+#pragma unroll
+  for (int i = 0; i < kFmaChains; ++i) a[i] = make_float2(1.f + 1e-3f * i, 1.f - 1e-3f * i + 1e-7f * threadIdx.x);
+  const float2 m = make_float2(0.999f, 0.999f), c = make_float2(0.001f, 0.001f);
+  for (int it = 0; it < iters; ++it)
+#pragma unroll
+    for (int i = 0; i < kFmaChains; ++i) a[i] = __ffma2_rn(a[i], m, c);
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < kFmaChains; ++i) s += a[i].x + a[i].y;
+  out[(long)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+Status measure_fma_rates(int device, double* ffma_tflops, double* ffma2_tflops) {
+  TOTEM_CUDA(cudaSetDevice(device));
+  int sms = 0;
+  TOTEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  constexpr int threads = 256, per_sm = 8, iters = 1 << 16;
+  const int blocks = sms * per_sm;
+  float* out = nullptr;
+  TOTEM_CUDA(cudaMalloc(&out, sizeof(float) * blocks * threads));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto rate = [&](bool packed, double* tflops) -> Status {
+    float best = 0.f;
+    for (int rep = 0; rep < 4; ++rep) {  // the first launch is the warm-up
+      TOTEM_CUDA(cudaEventRecord(e0));
+      if (packed) k_fma2_rate<<<blocks, threads>>>(out, iters);
+      else k_fma_rate<<<blocks, threads>>>(out, iters);
+      TOTEM_CUDA(cudaGetLastError());
+      TOTEM_CUDA(cudaEventRecord(e1));
+      TOTEM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      TOTEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0 && (best == 0.f || ms < best)) best = ms;
+    }
+    const double fmas = (double)blocks * threads * iters * kFmaChains * (packed ? 2 : 1);
+    *tflops = 2.0 * fmas / (best * 1e-3) / 1e12;
+    return Status::Ok();
+  };
+  Status st = rate(false, ffma_tflops);
+  if (st.ok()) st = rate(true, ffma2_tflops);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  return st;
+}
+
 }  // namespace totem
