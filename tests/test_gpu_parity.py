@@ -154,9 +154,9 @@ def test_invalid_window_rejected(engine_lib):
 
 
 def test_path_used_is_reported_and_fused_only_refuses_cufft(engine_lib):
-    # an 80^2 window on a 160^2 grid: no hand-written transform of these lengths, so the fused
+    # an 80^2 window on a 176^2 grid: no hand-written transform of these lengths, so the fused
     # request runs on cuFFT, says so in its timing, and TOTEM_PATH_FUSED_ONLY refuses it
-    odd = request.build_small_stem(n=80, p=160, raster=(2, 2), step=5, slices=3, mid_layer=(2,))
+    odd = request.build_small_stem(n=80, p=176, raster=(2, 2), step=5, slices=3, mid_layer=(2,))
     s = capi.Session()
     s.upload(odd)
     s.run(path=capi.PATH_FUSED)
@@ -283,3 +283,20 @@ def test_mixed_radix_zero_band_skip_and_server(engine_lib, n, p):
     np.testing.assert_array_equal(r1, outs[True][0])
     np.testing.assert_array_equal(m1, outs[True][1])
     _check(req, *outs[True], T=capi.transmission_run(req) if p > 1024 else None)
+
+
+@pytest.mark.parametrize("p", [320, 400, 576])
+def test_mixed_radix_potential_grid_transmission(engine_lib, p):
+    # mixed-radix potential grids take the fused transmission FFT (TOTEM_PATH_FUSED_ONLY accepts them)
+    req = request.build_small_stem(n=64, p=p, raster=(2, 2), step=9, slices=3, sampling=max(0.05, 20.0 / p),
+                                   cells=4, mid_layer=(2,))
+    s = capi.Session()
+    s.upload(req)
+    s.run(path=capi.PATH_FUSED_ONLY)
+    t = s.timing()
+    assert (t.slice_path, t.tx_fft_path) == (capi.PATH_FUSED, capi.PATH_FUSED)
+    res, mid, _ = s.download()
+    s.close()
+    ref_t = so.transmission(req)
+    assert rel_l2(capi.transmission_run(req), ref_t) < TOL
+    _check(req, res, mid, T=ref_t)

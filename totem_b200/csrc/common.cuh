@@ -145,7 +145,14 @@ Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sigma
 // Element-wise (-1)^(r+c) and exp for the cuFFT builder.
 Status launch_sign_exp(float2* data, long total, int p_h, int p_w, float sigma_scaled, cudaStream_t st);
 
+// Grid edges of the fused transmission FFT (powers of two 64..4096 and the mixed-radix edges of
+// TOTEM_MR_WINDOWS), and of the gridding builder (powers of two 64..4096).
 bool fused_fft_size_ok(int n);
+bool gridding_size_ok(int n);
+// Whether the fused transmission FFT takes a p_h x p_w grid of ``slices`` slices: both edges
+// fused_fft_size_ok, the rows of all slices whole row tiles of p_w and the width whole column
+// tiles of p_h.
+bool tx_fft_shape_ok(int p_h, int p_w, int slices);
 // Per-stage twiddle tables of the shared-memory FFT of length n (empty if n is unsupported).
 std::vector<float2> stage_twiddles(int n);
 
@@ -268,6 +275,11 @@ struct WindowOps {
   // HRTEM imaging (launch_exit_wave / launch_tcc_image semantics: out_i == nullptr for the exit wave)
   Status (*image)(const float2* spec, const float2* tf, int planes, const double* w, float2* work, float2* out_c,
                   float* out_i, const float2* tw, cudaStream_t st);
+  int row_tile_rows;     // RowCfg<n>::G
+  int col_tile_cols;     // the transmission column pass's tile width (GridColCfg<n>::G)
+  // the transmission's inverse FFT: rows of length n, then columns of length n with the sign and exp
+  Status (*tx_rows_inv)(float2* data, long nrows, const float2* tw, cudaStream_t st);
+  Status (*tx_cols_exp)(float2* data, int slices, int p_w, const float2* tw, float sig, cudaStream_t st);
 };
 const WindowOps* radix_window_ops(int n);
 

@@ -472,10 +472,11 @@ Status totem_session::upload_args(const TotemStemArgs* a, bool stem) {
 // ---------------------------------------------------------------------------------------------
 Status totem_session::build_transmission(int path, int* launches) {
   const size_t plane = (size_t)p_h * p_w;
-  const bool fft_fused = totem::fused_fft_size_ok(p_h) && totem::fused_fft_size_ok(p_w);
+  const bool fft_fused = totem::tx_fft_shape_ok(p_h, p_w, std::max(slices, 1));
   if (path == TOTEM_PATH_FUSED_ONLY && !fft_fused && slices > 0)
     return Status::Err(TOTEM_ERR_UNSUPPORTED,
-                       "TOTEM_PATH_FUSED_ONLY: the transmission FFT needs a power-of-two potential grid of 64..4096");
+                       "TOTEM_PATH_FUSED_ONLY: the transmission FFT needs a potential grid edge of 64..4096 that is a power "
+                       "of two, or a mixed-radix edge");
   TOTEM_TRY(T.ensure(plane * std::max(slices, 1) * sizeof(float2)));
   if (slices == 0) return Status::Ok();
   totem::TxGrid g;
@@ -572,7 +573,7 @@ Status totem_session::plan_gridding(const TotemStemArgs* a, const totem::Species
   grid_job_beg_h.clear();
   grid_jobs_h.clear();
   grid_atoms = 0;
-  if (!totem::fused_fft_size_ok(p_h) || !totem::fused_fft_size_ok(p_w) || slices <= 0) return Status::Ok();
+  if (!totem::gridding_size_ok(p_h) || !totem::gridding_size_ok(p_w) || slices <= 0) return Status::Ok();
   auto uniform = [](const double* v, int n, long stride, double* d) {
     *d = (v[(long)(n - 1) * stride] - v[0]) / (n - 1);
     if (!std::isfinite(*d) || *d == 0.0) return false;

@@ -3,6 +3,7 @@
 // groups.cu; mixed-radix windows: windows_mixed_*.cu).
 #pragma once
 #include "hrtem_kernels.cuh"
+#include "tx_fft.cuh"
 #include "slice_tiles.cuh"
 
 namespace totem {
@@ -228,7 +229,11 @@ const WindowOps* window_ops() {
                              &row_groups<N>,
                              &col_groups<N>,
                              &tables<N>,
-                             &image_n<N>};
+                             &image_n<N>,
+                             RowCfg<N>::G,
+                             GridColCfg<N>::G,
+                             &rows_inv<N>,
+                             &cols_exp<N>};
   return &ops;
 }
 

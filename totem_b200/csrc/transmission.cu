@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "tx_fft.cuh"
 
 namespace totem {
 
@@ -437,10 +438,6 @@ __global__ void __launch_bounds__(GridRowCfg<N>::G * GridRowCfg<N>::T, GridRowCf
   }
 }
 
-// Column shape of the builder's transforms: columns of 4096 take four per CTA (32-byte row
-// segments, whole sectors; 168 KB of shared memory), shorter ones the default width.
-template <int N>
-using GridColCfg = ColCfg<N, 4, (N == 4096) ? 4 : 0>;
 // Forward FFT of the columns of pitched planes (width columns, rows ``pitch`` apart).  Plane pl is
 // (job pl / 2, parity ey = pl % 2); its row q is fine row 2 q + ey, which is zero when no atom
 // touched it (row_used == 0: the row pass left the cleared zeros there), so it is not read.
@@ -530,58 +527,6 @@ Status grid_cols(float2* data, long planes, int width, long pitch, long plane_st
   return cuda_status(cudaGetLastError(), "k_grid_cols");
 }
 
-// In-place inverse FFT of rows of length N (RowCfg<N>::G rows per CTA).
-template <int N>
-__global__ void __launch_bounds__(RowCfg<N>::G * RowCfg<N>::T, RowCfg<N>::MINB) k_fft_rows_inv(float2* __restrict__ data,
-                                                                             const float2* __restrict__ tw) {
-  constexpr int P = RowCfg<N>::P, T = RowCfg<N>::T, G = RowCfg<N>::G;
-  extern __shared__ float2 sh[];
-  float2* s_tw = sh;
-  float2* s_x = sh + Fft<N>::tw_size;
-  const int g = threadIdx.x / T, j = threadIdx.x - g * T;
-  const long row = (long)blockIdx.x * G + g;
-  load_twiddles<N>(s_tw, tw);
-  float2* p = data + row * N;
-  float2 v[P];
-#pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = p[j + m * T];
-  __syncthreads();
-  fft_regs<N, true>(v, j, g, s_tw, s_x, RowLayout<N>(), group_sync<N>(g));
-#pragma unroll
-  for (int m = 0; m < P; ++m) p[j + m * T] = v[m];
-}
-
-// Column inverse FFT of length N over a p_w-wide plane, (-1)^(r+c), exp(i s V).
-template <int N>
-__global__ void __launch_bounds__(GridColCfg<N>::G * GridColCfg<N>::T, GridColCfg<N>::MINB) k_fft_cols_exp(float2* __restrict__ data, int p_w,
-                                                                             const float2* __restrict__ tw, float sig) {
-  constexpr int P = GridColCfg<N>::P, T = GridColCfg<N>::T, G = GridColCfg<N>::G;
-  extern __shared__ float2 sh[];
-  float2* s_tw = sh;
-  float2* s_x = sh + Fft<N>::tw_size;
-  const int j = threadIdx.x / G, g = threadIdx.x - j * G;
-  const int nblk = p_w / G;
-  const int slice = blockIdx.x / nblk, cb = blockIdx.x - slice * nblk;
-  const int c = cb * G + g;
-  load_twiddles<N>(s_tw, tw);
-  float2* p = data + (long)slice * N * p_w + c;
-  float2 v[P];
-#pragma unroll
-  for (int m = 0; m < P; ++m) v[m] = p[(long)(j + m * T) * p_w];
-  __syncthreads();
-  fft_regs<N, true>(v, j, g, s_tw, s_x, ColLayout<N, G>(), SyncBlock());
-#pragma unroll
-  for (int m = 0; m < P; ++m) {
-    const int r = j + m * T;
-    const float sgn = ((r + c) & 1) ? -1.f : 1.f;
-    const float re = sgn * v[m].x * sig, im = sgn * v[m].y * sig;
-    const float amp = expf(-im);
-    float sn, cs;
-    sincosf(re, &sn, &cs);
-    p[(long)r * p_w] = make_float2(amp * cs, amp * sn);
-  }
-}
-
 __global__ void k_sign_exp(float2* __restrict__ data, long total, int p_h, int p_w, float sig) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
     const long plane = (long)p_h * p_w;
@@ -599,29 +544,32 @@ __global__ void k_sign_exp(float2* __restrict__ data, long total, int p_h, int p
   }
 }
 
-template <int N>
-Status rows_inv(float2* data, long nrows, const float2* tw, cudaStream_t st) {
-  constexpr int T = RowCfg<N>::T, G = RowCfg<N>::G;
-  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + RowLayout<N>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_fft_rows_inv<N>, smem));
-  if (nrows % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "row count not a multiple of the row tile");
-  k_fft_rows_inv<N><<<(unsigned)(nrows / G), G * T, smem, st>>>(data, tw);
-  return cuda_status(cudaGetLastError(), "k_fft_rows_inv");
-}
-
-template <int N>
-Status cols_exp(float2* data, int slices, int p_w, const float2* tw, float sig, cudaStream_t st) {
-  constexpr int T = GridColCfg<N>::T, G = GridColCfg<N>::G;
-  const size_t smem = sizeof(float2) * (Fft<N>::tw_size + ColLayout<N, G>::size(G));
-  TOTEM_TRY(ensure_smem((const void*)k_fft_cols_exp<N>, smem));
-  if (p_w % G) return Status::Err(TOTEM_ERR_UNSUPPORTED, "potential width not a multiple of the column tile");
-  k_fft_cols_exp<N><<<(unsigned)((long)slices * (p_w / G)), G * T, smem, st>>>(data, p_w, tw, sig);
-  return cuda_status(cudaGetLastError(), "k_fft_cols_exp");
-}
-
 }  // namespace
 
-bool fused_fft_size_ok(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; }
+bool gridding_size_ok(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; }
+bool fused_fft_size_ok(int n) { return gridding_size_ok(n) || radix_window_ops(n) != nullptr; }
+
+namespace {
+template <int N>
+constexpr int2 tx_tiles() { return make_int2(RowCfg<N>::G, GridColCfg<N>::G); }
+// (rows per row tile, columns per column tile) of the transmission FFT at edge n; (0, 0) if none
+int2 tx_tiles_of(int n) {
+  switch (n) {
+#define TOTEM_TX_TILES(NN) \
+  case NN: return tx_tiles<NN>();
+    TOTEM_TX_TILES(64) TOTEM_TX_TILES(128) TOTEM_TX_TILES(256) TOTEM_TX_TILES(512) TOTEM_TX_TILES(1024)
+    TOTEM_TX_TILES(2048) TOTEM_TX_TILES(4096)
+#undef TOTEM_TX_TILES
+  }
+  if (const WindowOps* o = radix_window_ops(n)) return make_int2(o->row_tile_rows, o->col_tile_cols);
+  return make_int2(0, 0);
+}
+}  // namespace
+
+bool tx_fft_shape_ok(int p_h, int p_w, int slices) {
+  const int2 rw = tx_tiles_of(p_w), ch = tx_tiles_of(p_h);
+  return rw.x > 0 && ch.y > 0 && ((long)slices * p_h) % rw.x == 0 && p_w % ch.y == 0;
+}
 
 Status launch_tx_structure(const TxGrid& g, const AtomRowsDev& neutral, const AtomRowsDev& ion,
                            const AtomRowsDev& corr_n, const AtomRowsDev& corr_i, float2* out, cudaStream_t st,
@@ -681,7 +629,7 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesSet& sp, const GridPlanD
                           const float2* tw_h, void* scratch, size_t scratch_bytes, bool scratch_zero, float2* out,
                           cudaStream_t st, int* launches) {
   if (g.slices == 0) return Status::Ok();
-  if (!fused_fft_size_ok(g.p_h) || !fused_fft_size_ok(g.p_w))
+  if (!gridding_size_ok(g.p_h) || !gridding_size_ok(g.p_w))
     return Status::Err(TOTEM_ERR_UNSUPPORTED, "gridding builder needs power-of-two grids 64..4096");
   if ((int)job_beg.size() != g.slices + 1) return Status::Err(TOTEM_ERR_STATE, "gridding job table size");
   const long plane = (long)g.p_h * g.p_w;
@@ -743,28 +691,25 @@ Status launch_tx_gridding(const TxGrid& g, const SpeciesSet& sp, const GridPlanD
 
 Status launch_tx_fft_exp(float2* data, int slices, int p_h, int p_w, float sig, const float2* tw_w,
                          const float2* tw_h, cudaStream_t st) {
-  if (!fused_fft_size_ok(p_h) || !fused_fft_size_ok(p_w))
-    return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused transmission builder needs power-of-two grids 64..4096");
+  if (!tx_fft_shape_ok(p_h, p_w, slices))
+    return Status::Err(TOTEM_ERR_UNSUPPORTED, "fused transmission FFT: unsupported grid shape");
   const long nrows = (long)slices * p_h;
   switch (p_w) {
-    case 64: TOTEM_TRY(rows_inv<64>(data, nrows, tw_w, st)); break;
-    case 128: TOTEM_TRY(rows_inv<128>(data, nrows, tw_w, st)); break;
-    case 256: TOTEM_TRY(rows_inv<256>(data, nrows, tw_w, st)); break;
-    case 512: TOTEM_TRY(rows_inv<512>(data, nrows, tw_w, st)); break;
-    case 1024: TOTEM_TRY(rows_inv<1024>(data, nrows, tw_w, st)); break;
-    case 2048: TOTEM_TRY(rows_inv<2048>(data, nrows, tw_w, st)); break;
-    case 4096: TOTEM_TRY(rows_inv<4096>(data, nrows, tw_w, st)); break;
+#define TOTEM_TX_ROWS_CASE(NN) \
+  case NN: TOTEM_TRY(rows_inv<NN>(data, nrows, tw_w, st)); break;
+    TOTEM_TX_ROWS_CASE(64) TOTEM_TX_ROWS_CASE(128) TOTEM_TX_ROWS_CASE(256) TOTEM_TX_ROWS_CASE(512)
+    TOTEM_TX_ROWS_CASE(1024) TOTEM_TX_ROWS_CASE(2048) TOTEM_TX_ROWS_CASE(4096)
+#undef TOTEM_TX_ROWS_CASE
+    default: TOTEM_TRY(radix_window_ops(p_w)->tx_rows_inv(data, nrows, tw_w, st));
   }
   switch (p_h) {
-    case 64: return cols_exp<64>(data, slices, p_w, tw_h, sig, st);
-    case 128: return cols_exp<128>(data, slices, p_w, tw_h, sig, st);
-    case 256: return cols_exp<256>(data, slices, p_w, tw_h, sig, st);
-    case 512: return cols_exp<512>(data, slices, p_w, tw_h, sig, st);
-    case 1024: return cols_exp<1024>(data, slices, p_w, tw_h, sig, st);
-    case 2048: return cols_exp<2048>(data, slices, p_w, tw_h, sig, st);
-    case 4096: return cols_exp<4096>(data, slices, p_w, tw_h, sig, st);
+#define TOTEM_TX_COLS_CASE(NN) \
+  case NN: return cols_exp<NN>(data, slices, p_w, tw_h, sig, st);
+    TOTEM_TX_COLS_CASE(64) TOTEM_TX_COLS_CASE(128) TOTEM_TX_COLS_CASE(256) TOTEM_TX_COLS_CASE(512)
+    TOTEM_TX_COLS_CASE(1024) TOTEM_TX_COLS_CASE(2048) TOTEM_TX_COLS_CASE(4096)
+#undef TOTEM_TX_COLS_CASE
   }
-  return Status::Err(TOTEM_ERR_UNSUPPORTED, "grid size");
+  return radix_window_ops(p_h)->tx_cols_exp(data, slices, p_w, tw_h, sig, st);
 }
 
 Status launch_sign_exp(float2* data, long total, int p_h, int p_w, float sig, cudaStream_t st) {
