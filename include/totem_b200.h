@@ -59,8 +59,9 @@ enum { TOTEM_PARAM_PENG = 0,   /* rows of 13 (neutral) / 25 (ionic) columns */
 
 /* Slice-loop implementation.  TOTEM_PATH_FUSED runs the hand-written kernels where they apply
  * (square windows of 64..2048 for the slice loop: powers of two and the mixed-radix edges 96, 160,
- * 192, 288, 320, 384, 400, 448, 576, 640, 768, 800, 1152, 1280, 1536, 1600; power-of-two potential
- * grids of 64..4096 for the transmission FFT) and cuFFT elsewhere; TotemTiming reports what ran.
+ * 192, 288, 320, 384, 400, 448, 576, 640, 768, 800, 1152, 1280, 1536, 1600; potential grids of
+ * 64..4096 whose edges are powers of two or those mixed-radix edges, in whole row and column tiles,
+ * for the transmission FFT) and cuFFT elsewhere; TotemTiming reports what ran.
  * TOTEM_PATH_FUSED_ONLY fails with TOTEM_ERR_UNSUPPORTED instead of using cuFFT. */
 enum { TOTEM_PATH_FUSED = 0,      /* shared-memory FFT passes fused with the multiplies and detectors */
        TOTEM_PATH_PLAIN = 1,      /* cuFFT plus separate element-wise kernels (comparator)           */
