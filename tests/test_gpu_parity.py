@@ -300,3 +300,27 @@ def test_mixed_radix_potential_grid_transmission(engine_lib, p):
     ref_t = so.transmission(req)
     assert rel_l2(capi.transmission_run(req), ref_t) < TOL
     _check(req, res, mid, T=ref_t)
+
+
+@pytest.mark.parametrize("p_w,fused", [(160, False), (256, True)])
+def test_non_square_potential_grid(engine_lib, p_w, fused):
+    # A 192 x p_w potential grid: the fused transmission FFT needs the rows of all slices to make
+    # whole row tiles of p_w (20 rows for 160: 3 x 192 rows do not) and p_w whole column tiles of
+    # 192; otherwise the request runs the transmission FFT on cuFFT.  Both match the oracle.
+    from dataclasses import replace
+    from totem_b200 import optics
+    req = request.build_small_stem(n=64, p=192, raster=(2, 2), step=9, slices=3, sampling=0.1, mid_layer=(2,))
+    kx, ky, s2 = optics.reciprocal_grids(192, p_w, 0.1)
+    req = replace(req, p_width=p_w, kx=kx, ky=ky, s2=s2, aper_true=np.ones((192, p_w)),
+                  parameter=optics.potential_parameter(192, p_w, 0.1))
+    s = capi.Session()
+    s.upload(req)
+    s.run()
+    t = s.timing()
+    assert t.slice_path == capi.PATH_FUSED
+    assert t.tx_fft_path == (capi.PATH_FUSED if fused else capi.PATH_PLAIN)
+    res, mid, _ = s.download()
+    s.close()
+    ref_t = so.transmission(req)
+    assert rel_l2(capi.transmission_run(req), ref_t) < TOL
+    _check(req, res, mid, T=ref_t)
