@@ -525,12 +525,16 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Launch shapes shared by the kernels that transform whole rows or whole columns.
 // Rows: G transforms of T threads per CTA (each transform inside one warp, or a named barrier
 // per transform when T > 32), at most 32 KB of exchange space per CTA.
-// Rows per CTA: the largest g up to the cap (256 threads, or 4096 elements) that divides N (a
-// CTA's rows belong to one probe) and makes whole warps; for power-of-two N the cap itself.
+// Rows per CTA: the largest g up to the cap (256 threads below N = 256, 128 from there, or 4096
+// elements) that divides N (a CTA's rows belong to one probe) and makes whole warps; for
+// power-of-two N the cap itself.  At 256^2 the 128-thread CTA (8 rows) made the slice loop 3.7 %
+// faster than 16 rows (0.364 against 0.378 us per probe*slice); halving the rows at 512, 1024 and
+// 2048 made it 4, 4 and 14 % slower.
 template <int N>
 constexpr int row_group_count() {
   constexpr int T = Fft<N>::T;
-  constexpr int cap = (256 / T < 4096 / N) ? 256 / T : (4096 / N > 0 ? 4096 / N : 1);
+  constexpr int threads = N >= 256 ? 128 : 256;
+  constexpr int cap = (threads / T < 4096 / N) ? threads / T : (4096 / N > 0 ? 4096 / N : 1);
   for (int g = cap > 0 ? cap : 1; g >= 1; --g)
     if (N % g == 0 && (g * T) % 32 == 0) return g;
   for (int g = (cap > 0 ? cap : 1) + 1; g <= 64; ++g)
