@@ -562,7 +562,8 @@ template <int N, int CTAS128 = 4, int GW = 0>
 struct ColCfg {
   static constexpr int P = Fft<N>::P, T = Fft<N>::T;
   // GW = 0: the default width, 16 columns (one 128-byte segment per row) up to N = 512, 8 (64
-  // bytes) up to 2048 (at 2048 one 512-thread CTA per SM; 4 columns at two CTAs was 10 % slower)
+  // bytes) up to 2048 (at 2048 one 512-thread CTA per SM; 4 columns at two CTAs was 10 % slower;
+  // at 1024 4-column tiles at four 128-thread CTAs per SM made the column pass 23 % slower)
   static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 2048 ? 8 : 2));
   static_assert((G * T) % 32 == 0 && N % G == 0, "column tile: whole warps, whole tiles");
   // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
