@@ -13,7 +13,8 @@
 // butterflies run in registers as 4x4 and 8x4 Cooley-Tukey splits whose internal twiddles are
 // compile-time constants.  Mixed-radix windows (96 .. 1600, TOTEM_PLAN below) add radices with
 // a factor 3, 5 or 7 (odd primes from the DFT definition folded over conjugate pairs, composites
-// such as 24 = 8 x 3 by the same Cooley-Tukey split); their T = N / P need not be a power of two.  Inter-stage twiddles W_N^e = exp(-2 pi i e / N) come from per-stage
+// such as 24 = 8 x 3 by the same Cooley-Tukey split); their T = N / P need not be a power of two.
+// Inter-stage twiddles W_N^e = exp(-2 pi i e / N) come from per-stage
 // tables (index (r-1)*Ns + k) computed on the host in FP64, rounded once to FP32 and staged in
 // shared memory; lanes with consecutive k read consecutive entries, so the reads are free of bank
 // conflicts.  Exchanges use XOR-swizzled addresses chosen so that every 64-bit store and load of
