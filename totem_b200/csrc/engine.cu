@@ -475,8 +475,8 @@ Status totem_session::build_transmission(int path, int* launches) {
   const bool fft_fused = totem::tx_fft_shape_ok(p_h, p_w, std::max(slices, 1));
   if (path == TOTEM_PATH_FUSED_ONLY && !fft_fused && slices > 0)
     return Status::Err(TOTEM_ERR_UNSUPPORTED,
-                       "TOTEM_PATH_FUSED_ONLY: the transmission FFT needs a potential grid edge of 64..4096 that is a power "
-                       "of two, or a mixed-radix edge");
+                       "TOTEM_PATH_FUSED_ONLY: the transmission FFT needs potential grid edges of 64..4096 "
+                       "that are powers of two or mixed-radix edges, in whole tiles");
   TOTEM_TRY(T.ensure(plane * std::max(slices, 1) * sizeof(float2)));
   if (slices == 0) return Status::Ok();
   totem::TxGrid g;

@@ -718,7 +718,8 @@ int totem_server_submit(totem_server* s, const TotemStemArgs* args, TotemStemOut
   Status st = totem_session::validate(args, true);
   if (!st.ok()) return server_fail(st);
   if (args->depth > 0 && !fused_window(args->height, args->width))
-    return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server runs square windows of 64..2048: powers of two or the mixed-radix edges"));
+    return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED,
+                                   "the server runs square windows of 64..2048: powers of two or the mixed-radix edges"));
   if (args->depth > 0 && args->slices < 1)
     return server_fail(Status::Err(TOTEM_ERR_UNSUPPORTED, "the server needs at least one slice"));
   std::unique_ptr<Request> r(new Request());
