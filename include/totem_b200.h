@@ -354,6 +354,19 @@ TOTEM_API int totem_session_hrtem(totem_session *s, const TotemHrtemArgs *h, Tot
 TOTEM_API int totem_hrtem_run(const TotemStemArgs *specimen, const TotemHrtemArgs *h, TotemHrtemOut *out);
 
 /* ---------------------------------------------------------------------------------------------
+ * CBED: the convergent-beam diffraction pattern of one probe position.  The reference builds the
+ * transmission with the *P MEX and runs this part in MATLAB (ToTEM_submit_v1.m:1478-1492): per
+ * defocus probe n, psi = probe_n; per slice psi = ifft2(fft2(psi .* T_k[window]) .* psf_fft);
+ * pattern = sum_n gfsf_n |fftshift(fft2(psi))|^2.  The request is a STEM request with depth 1: the
+ * probes (w_num), the propagator, gfsf and the window origin begin_row / begin_col (0-based) are
+ * used; the detector fields are not (aper_num may be 0).  ``pattern`` receives height x width
+ * doubles, row-major, zero frequency at the centre.  Windows of the fused slice loop run the fused
+ * passes, other windows cuFFT; totem_session_timing's slice_path says which.
+ * ------------------------------------------------------------------------------------------- */
+TOTEM_API int totem_session_cbed(totem_session *s, double *pattern);
+TOTEM_API int totem_cbed_run(const TotemStemArgs *request, double *pattern);
+
+/* ---------------------------------------------------------------------------------------------
  * Probe / image transfer functions (WholeTCC2D_newTEM, ToTEM_submit_v1.m:2305-2406), evaluated on
  * the current device in FP64.  The reference computes them in MATLAB for every request.
  * ------------------------------------------------------------------------------------------- */

@@ -240,6 +240,28 @@ def _origins(req):
 
 
 # ----------------------------------------------------------------------------------------------
+# CBED: one probe position, the whole diffraction pattern (ToTEM_submit_v1.m:1478-1492)
+# ----------------------------------------------------------------------------------------------
+
+def cbed(req, T: np.ndarray | None = None) -> np.ndarray:
+    """sum_n gfsf_n |fftshift(fft2(psi_n))|^2 over the defocus probes, psi_n propagated from the
+    probe window at (beginrow, begincol) through every slice: psi .* T_k window, fft2, .* psf,
+    ifft2 (the loop of ToTEM_submit_v1.m:1481-1491).  Returns the [H, W] pattern, zero frequency
+    at the centre."""
+    if T is None:
+        T = transmission(req)
+    r0, c0 = int(req.beginrow), int(req.begincol)
+    out = np.zeros((req.height, req.width))
+    for w in range(req.w_num):
+        psi = np.asarray(req.probe[w], dtype=np.complex128)
+        for k in range(T.shape[0]):
+            psi = psi * T[k, r0:r0 + req.height, c0:c0 + req.width]
+            psi = sfft.ifft2(sfft.fft2(psi) * req.prop)
+        out += req.gfsf[w] * np.abs(np.fft.fftshift(sfft.fft2(psi))) ** 2
+    return out
+
+
+# ----------------------------------------------------------------------------------------------
 # HRTEM plane-wave multislice (ToTEM_submit_v1.m:1320-1369)
 # ----------------------------------------------------------------------------------------------
 

@@ -142,3 +142,21 @@ def test_focal_spread_steps_must_be_odd():
         optics.gaussian_focal_weights(2, 4.0, 0.0025, 1.0)
     d, w = optics.gaussian_focal_weights(3, 4.0, 0.0025, 1.0)
     assert len(w) == 3 and d > 0
+
+
+def test_cbed_in_vacuum_is_the_probe_spectrum():
+    # With T = 1 every slice only multiplies the spectrum by the unit-modulus propagator inside its
+    # band, and the probes (20 mrad aperture) lie inside it: the CBED pattern is
+    # sum_n gfsf_n |fftshift(fft2(probe_n))|^2 (ToTEM_submit_v1.m:1478-1492), whose sum is
+    # N^2 sum_n gfsf_n |probe_n|^2 (Parseval).
+    req = request.build_small_stem(n=64, p=128, raster=(1, 1), slices=4, focal_steps=3)
+    T = np.ones((req.slices, req.p_height, req.p_width), dtype=np.complex128)
+    pat = so.cbed(req, T)
+    ref = sum(g * np.abs(np.fft.fftshift(np.fft.fft2(p))) ** 2 for g, p in zip(req.gfsf, req.probe))
+    assert rel_l2(pat, ref) < 1e-12
+    norm = sum(g * np.sum(np.abs(p) ** 2) for g, p in zip(req.gfsf, req.probe))
+    assert abs(pat.sum() / (req.height * req.width * norm) - 1.0) < 1e-12
+    # zero frequency at the centre: the untilted bright-field disc is centred on (N/2, N/2)
+    r, c = np.indices(pat.shape)
+    assert abs((r * pat).sum() / pat.sum() - req.height // 2) < 0.5
+    assert abs((c * pat).sum() / pat.sum() - req.width // 2) < 0.5

@@ -170,7 +170,7 @@ def load() -> C.CDLL:
     for name in ("totem_session_create", "totem_session_destroy", "totem_session_upload", "totem_session_run",
                  "totem_session_download", "totem_session_timing", "totem_session_transmission",
                  "totem_stem_run", "totem_transmission_run", "totem_stem_slices_noalloc", "totem_session_hrtem",
-                 "totem_hrtem_run", "totem_server_create",
+                 "totem_hrtem_run", "totem_session_cbed", "totem_cbed_run", "totem_server_create",
                  "totem_server_submit", "totem_server_wait", "totem_server_info", "totem_server_destroy",
                  "totem_server_stats", "totem_plan_simulate", "totem_tcc_stack", "totem_set_tx_builder",
                  "totem_grid_batches", "totem_set_slice_graphs", "totem_set_band_skip", "totem_fp32_peak", "totem_inject_failures", "totem_load_tuning", "totem_tuned_config", "totem_slice_rows", "totem_fold_debye_waller", "totem_frozen_phonon"):
@@ -298,6 +298,12 @@ class Session:
         h, out, ex, img = _hrtem_marshal(spec, self.req.p_height, self.req.p_width, t_storage, exit_wave, image)
         check(self.lib.totem_session_hrtem(self.h, C.byref(h.args), C.byref(out)))
         return ex(), img
+
+    def cbed(self):
+        """CBED pattern of the uploaded depth-1 request (``totem_session_cbed``)."""
+        pat = np.zeros(self.req.height * self.req.width)
+        check(self.lib.totem_session_cbed(self.h, _ptr(pat)))
+        return pat.reshape(self.req.height, self.req.width)
 
     def download(self, want_transmission: bool = False):
         req = self.req
@@ -479,6 +485,16 @@ def hrtem_run(specimen, spec, t_storage: int = T_COMPLEX64, exit_wave: bool = Tr
     h, out, ex, img = _hrtem_marshal(spec, specimen.p_height, specimen.p_width, t_storage, exit_wave, image)
     check(lib.totem_hrtem_run(C.byref(m.args), C.byref(h.args), C.byref(out)))
     return ex(), img
+
+
+def cbed_run(req):
+    """One-shot CBED pattern (``totem_cbed_run``) of a depth-1 request: [height, width], zero
+    frequency at the centre."""
+    lib = load()
+    m = Marshalled(req, True)
+    pat = np.zeros(req.height * req.width)
+    check(lib.totem_cbed_run(C.byref(m.args), _ptr(pat)))
+    return pat.reshape(req.height, req.width)
 
 
 def stem_run(req, path: int = PATH_FUSED, batch: int = 0):

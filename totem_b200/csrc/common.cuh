@@ -311,6 +311,9 @@ Status launch_plain_scale(float2* psi, float s, long total, cudaStream_t st);
 Status launch_plain_tf_mul(float2* work, const float2* spec, const float2* tf, int vol, int planes, cudaStream_t st);
 Status launch_plain_image(const float2* work, int planes, const double* w, float s, int vol, float* out,
                           cudaStream_t st);
+// CBED: out[h][w] = sum_q gfsf[q] |fftshift(spec_q)|^2 over w_num kept spectra [w_num][h][w] (FP64).
+Status launch_cbed_pattern(const float2* spec, const double* gfsf, int w_num, int h, int w, double* out,
+                           cudaStream_t st);
 Status launch_plain_detect(const float2* psi, const float* masks, int aper_num, int vol, int items,
                            double* part, int nblk, cudaStream_t st);
 

@@ -1042,6 +1042,61 @@ Status totem_session::hrtem_plain(const TotemHrtemArgs* hr, TotemHrtemOut* out, 
   return Status::Ok();
 }
 
+// CBED (ToTEM_submit_v1.m:1478-1492): the uploaded probes (w_num defocus probes, one scan
+// position) through every slice, and sum_w gfsf_w |fftshift(FFT2(psi_w))|^2.  The final FFT2 of
+// the reference follows an IFFT2 of the last slice's spectrum .* psf, so it is that spectrum: the
+// fused route keeps it from the last column pass (flag 8), the cuFFT route stops after its
+// multiply.
+Status totem_session::cbed(double* pattern) {
+  if (!uploaded || !stem_ready) return Status::Err(TOTEM_ERR_STATE, "CBED before the upload of a probe request");
+  if (pattern == nullptr) return Status::Err(TOTEM_ERR_INVALID_ARG, "pattern is NULL");
+  if (depth != 1) return Status::Err(TOTEM_ERR_INVALID_ARG, "CBED takes one probe position (depth 1)");
+  if (slices < 1) return Status::Err(TOTEM_ERR_INVALID_ARG, "CBED needs a slice");
+  TOTEM_CUDA(cudaSetDevice(device));
+  int launches = 0;
+  if (!t_valid) TOTEM_TRY(build_transmission(TOTEM_PATH_FUSED, &launches));
+  const size_t vol = (size_t)h * w;
+  const bool fused = h == w && totem::fused_window_ok(h);
+  TOTEM_TRY(psi.ensure((size_t)w_num * vol * sizeof(float2)));
+  const totem::ScanGeom geo{begin_row, begin_col, step, width_red, depth, p_w};
+  const float2* Tp = T.as<float2>();
+  const size_t plane = (size_t)p_h * p_w;
+  float2* ps = psi.as<float2>();
+  if (fused) {
+    totem::SliceLoopArgs s;
+    s.n = h; s.items = w_num; s.item0 = 0; s.geo = geo; s.p_h = p_h;
+    s.psi = ps; s.probe = probe.as<float2>(); s.prop = prop.as<float2>();
+    s.tw = tw_n.as<float2>(); s.aper_num = 0;
+    s.skip_band = (totem::band_skip_enabled() && totem::band_skip_ok(h, band, 0)) ? 1 : 0;
+    TOTEM_TRY(totem::launch_row_pass(s, Tp, true, stream));
+    for (int k = 0; k < slices; ++k) {
+      TOTEM_TRY(totem::launch_col_pass(s, k == slices - 1 ? 4 | 8 : 0, stream));
+      if (k < slices - 1) TOTEM_TRY(totem::launch_row_pass(s, Tp + (k + 1) * plane, false, stream));
+    }
+  } else {
+    cufftHandle p;
+    TOTEM_TRY(plan(h, w, w_num, &p));
+    TOTEM_TRY(totem::launch_plain_init(ps, probe.as<float2>(), h, w, w_num, 0, depth, stream));
+    for (int k = 0; k < slices; ++k) {
+      TOTEM_TRY(totem::launch_plain_gather_mul(ps, Tp + (size_t)k * plane, h, w, w_num, 0, geo, stream));
+      TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_FORWARD));
+      TOTEM_TRY(totem::launch_plain_mul(ps, prop.as<float2>(), (int)vol, w_num, stream));
+      if (k < slices - 1) {
+        TOTEM_CUFFT(cufftExecC2C(p, (cufftComplex*)ps, (cufftComplex*)ps, CUFFT_INVERSE));
+        TOTEM_TRY(totem::launch_plain_scale(ps, 1.f / (float)vol, (long)w_num * vol, stream));
+      }
+    }
+  }
+  TOTEM_TRY(cbed_out.ensure(vol * sizeof(double)));
+  TOTEM_TRY(totem::launch_cbed_pattern(ps, gfsf_d.as<double>(), w_num, h, w, cbed_out.as<double>(), stream));
+  TOTEM_CUDA(cudaMemcpyAsync(pattern, cbed_out.p, vol * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  TOTEM_CUDA(cudaStreamSynchronize(stream));
+  timing.slice_path = fused ? TOTEM_PATH_FUSED : TOTEM_PATH_PLAIN;
+  timing.tx_fft_path = ran_tx_fft;
+  timing.tx_builder = ran_tx_builder;
+  return Status::Ok();
+}
+
 Status totem_session::run(int what, const TotemRunOptions* opt) {
   if (!uploaded) return Status::Err(TOTEM_ERR_STATE, "run before a successful upload");
   TotemRunOptions o{};
@@ -1334,6 +1389,23 @@ int totem_hrtem_run(const TotemStemArgs* specimen, const TotemHrtemArgs* h, Tote
     TOTEM_CUDA(cudaSetDevice(s->device));
     TOTEM_TRY(s->upload_args(specimen, false));
     return s->hrtem(h, out);
+  });
+}
+
+int totem_session_cbed(totem_session* s, double* pattern) {
+  if (!s) return fail(Status::Err(TOTEM_ERR_INVALID_ARG, "session is NULL"));
+  std::lock_guard<std::mutex> lk(s->mu);
+  return guarded([&] { return s->cbed(pattern); });
+}
+
+int totem_cbed_run(const TotemStemArgs* args, double* pattern) {
+  return guarded([&]() -> Status {
+    totem_session* s = nullptr;
+    TOTEM_TRY(default_session(&s));
+    std::lock_guard<std::mutex> lk(s->mu);
+    TOTEM_CUDA(cudaSetDevice(s->device));
+    TOTEM_TRY(s->upload_args(args, true));
+    return s->cbed(pattern);
   });
 }
 

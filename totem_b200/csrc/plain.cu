@@ -99,6 +99,23 @@ __global__ void k_plain_image(const float2* __restrict__ work, int planes, const
   }
 }
 
+// CBED pattern: out[r][c] = sum_w gfsf[w] |spec_w[(r + h/2) % h][(c + w/2) % w]|^2 (fftshift of the
+// kept spectra, FP64, probes in ascending order).
+__global__ void k_cbed_pattern(const float2* __restrict__ spec, const double* __restrict__ gfsf, int w_num, int h,
+                               int w, double* __restrict__ out) {
+  const long vol = (long)h * w;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < vol; i += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / w), c = (int)(i % w);
+    const long src = (long)((r + h / 2) % h) * w + (c + w / 2) % w;
+    double acc = 0.0;
+    for (int q = 0; q < w_num; ++q) {
+      const float2 v = spec[(long)q * vol + src];
+      acc += gfsf[q] * ((double)v.x * v.x + (double)v.y * v.y);
+    }
+    out[i] = acc;
+  }
+}
+
 inline int grid_for(long total) { return (int)std::min<long>((total + 255) / 256, 148L * 32); }
 
 }  // namespace
@@ -148,6 +165,14 @@ Status launch_plain_image(const float2* work, int planes, const double* w, float
   if (vol == 0) return Status::Ok();
   k_plain_image<<<grid_for(vol), 256, 0, st>>>(work, planes, w, s, vol, out);
   return cuda_status(cudaGetLastError(), "k_plain_image");
+}
+
+Status launch_cbed_pattern(const float2* spec, const double* gfsf, int w_num, int h, int w, double* out,
+                           cudaStream_t st) {
+  const long vol = (long)h * w;
+  if (vol == 0) return Status::Ok();
+  k_cbed_pattern<<<grid_for(vol), 256, 0, st>>>(spec, gfsf, w_num, h, w, out);
+  return cuda_status(cudaGetLastError(), "k_cbed_pattern");
 }
 
 }  // namespace totem

@@ -185,6 +185,7 @@ struct totem_session {
   bool tb_valid = false;
   // HRTEM inputs and outputs
   totem::DevBuf hr_wave, hr_prop, hr_tf, hr_w, hr_work, hr_exit, hr_img;
+  totem::DevBuf cbed_out;  // the CBED pattern [H][W] (FP64)
   bool t_valid = false;
   bool has_result = false;
   int last_what = 0;
@@ -292,6 +293,7 @@ struct totem_session {
   void drop_graph();
   Status hrtem(const TotemHrtemArgs* h, TotemHrtemOut* out);
   Status hrtem_plain(const TotemHrtemArgs* hr, TotemHrtemOut* out, const float2* Tp);
+  Status cbed(double* pattern);
   Status run(int what, const TotemRunOptions* opt);
   Status collect_timing();
   Status download(TotemStemOut* out);
