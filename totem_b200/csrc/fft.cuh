@@ -565,7 +565,11 @@ struct ColCfg {
   // GW = 0: the default width, 16 columns (one 128-byte segment per row) up to N = 512, 8 (64
   // bytes) up to 2048 (at 2048 one 512-thread CTA per SM; 4 columns at two CTAs was 10 % slower;
   // at 1024 4-column tiles at four 128-thread CTAs per SM made the column pass 23 % slower)
-  static constexpr int G = GW ? GW : ((N <= 512) ? 16 : (N <= 2048 ? 8 : 2));
+  static constexpr int G0 = (N <= 512) ? 16 : (N <= 2048 ? 8 : 2);
+  // Mixed-radix windows whose tile would exceed 256 threads take half the columns when the half
+  // tile is still at most 256 threads (two CTAs per SM): 800^2 12 %, 1152^2 and 1536^2 3 % faster
+  // slice loops; at 1600^2 the half tile (320 threads, one CTA per SM) was 8 % slower.
+  static constexpr int G = GW ? GW : (((N & (N - 1)) && G0 * T > 256 && (G0 / 2) * T <= 256) ? G0 / 2 : G0);
   static_assert((G * T) % 32 == 0 && N % G == 0, "column tile: whole warps, whole tiles");
   // resident CTAs of 128 threads requested per SM (4 = a 128-register cap)
   static constexpr int MINB = (CTAS128 * 128 / (G * T) > 0) ? CTAS128 * 128 / (G * T) : 1;
