@@ -111,9 +111,12 @@ def test_plan_schedule_is_the_dft(n):
     p, radices = PLANS[n]
     assert int(np.prod(radices)) == n and all(p % r == 0 for r in radices) and len(radices) <= 3
     t = n // p
-    # launch shapes: a column tile of G columns x T threads is whole warps (G = 16 up to 512,
-    # 8 above); transform groups that do not divide a warp evenly synchronise the whole CTA
+    # launch shapes (ColCfg): a column tile of G columns x T threads is whole warps (G = 16 up to
+    # 512, 8 above; mixed-radix edges halve it when the tile exceeds 256 threads and the half tile
+    # does not); transform groups that do not divide a warp evenly synchronise the whole CTA
     g = 16 if n <= 512 else (8 if n <= 2048 else 2)
+    if n & (n - 1) and g * t > 256 and (g // 2) * t <= 256:
+        g //= 2
     assert (g * t) % 32 == 0 and n % g == 0
     rng = np.random.default_rng(n)
     x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
