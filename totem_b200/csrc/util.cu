@@ -135,6 +135,12 @@ __global__ void k_fma2_rate(float* __restrict__ out, int iters) {
 }  // namespace
 
 Status measure_fma_rates(int device, double* ffma_tflops, double* ffma2_tflops) {
+  int previous = 0;
+  TOTEM_CUDA(cudaGetDevice(&previous));
+  struct Restore {  // the caller's current device is left as it was, on every return
+    int dev;
+    ~Restore() { cudaSetDevice(dev); }
+  } restore{previous};
   TOTEM_CUDA(cudaSetDevice(device));
   int sms = 0;
   TOTEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
