@@ -96,11 +96,16 @@ def test_no_device_is_an_error_not_a_crash(lib):
     assert lib.totem_session_create(-1, None, C.byref(h)) == capi.ERR_NO_DEVICE
     a, b = C.c_double(), C.c_double()
     assert lib.totem_fp32_peak(0, C.byref(a), C.byref(b)) == capi.ERR_NO_DEVICE
+    one = request.build_small_stem(n=64, p=128, raster=(1, 1), slices=2)
+    with pytest.raises(capi.TotemError) as e:
+        capi.cbed_run(one)
+    assert e.value.code == capi.ERR_NO_DEVICE
 
 
 def test_null_arguments_are_rejected(lib):
     assert lib.totem_session_create(0, None, None) == capi.ERR_INVALID_ARG
     assert lib.totem_fp32_peak(0, None, None) == capi.ERR_INVALID_ARG
+    assert lib.totem_session_cbed(None, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_upload(None, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_run(None, 0, None) == capi.ERR_INVALID_ARG
     assert lib.totem_session_destroy(None) == capi.OK
